@@ -1,0 +1,405 @@
+"""Benchmark: particle-steps/s of the particle side of a PIC step on B200.
+
+One step = 5 fused LSRK4 stages (velocity, monomial interpolation, Lorentz
+force, RK update, element relocation) + one deposition of rho and j onto the
+DG nodes (+ the element sort of the store). Default workload: config2 --
+32x32x128 cubes x 6 jittered tets (786,432 tets), order 3 (Np = 20,
+15.7M nodes), 16M electrons in an r < 0.25 cm beam, shape-function
+deposition with radius 0.08 cm, static Bz + 8 seeded Fourier modes of E and
+B; FP64 plain form. Inputs are far larger than L2 (3.5 GB of particle state
+moved per stage), so no L2 flush is needed between steps.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+With N > 1 (torchrun), every rank advances its own 16M particles (weak
+scaling) and rho/j are summed across ranks with one NCCL all-reduce per step.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="config2")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_method(w, torch):
+    from pyrticle_b200.cloud import PicMethod
+    from pyrticle_b200.deposition.shape import ShapeFunctionDepositor
+    from pyrticle_b200.discretization import Discretization
+    from pyrticle_b200.pusher import MonomialParticlePusher
+    from pyrticle_b200.tools import PolynomialShapeFunction
+    from pyrticle_b200.units import SIUnitsWithNaturalConstants as U
+    discr = Discretization(w.mesh, w.order, nodes=w.nodes)
+    m = PicMethod(discr, U, ShapeFunctionDepositor(), MonomialParticlePusher(), 3, 3)
+    sf = PolynomialShapeFunction(w.shape_radius, 3, 2)
+    m.depositor.set_shape_function(None, sf)
+    return m, sf
+
+
+def count_pairs(m, state, sf):
+    """Exact number of (particle, node) pairs inside the radius (one call)."""
+    from pyrticle_b200 import _lib
+    import torch
+    nn = len(m.discretization)
+    rho = torch.empty((nn,), dtype=torch.float64, device="cuda")
+    st = _lib.DepositStats()
+    _lib.check(m.lib.prt_deposit_shape(
+        m.mesh_data.handle, m.workspace, _lib.DEPOSIT_PLAIN,
+        _lib.ShapeFunctionDesc(sf.radius, sf.exponent, sf.normalizer), None, len(state),
+        state.x.data_ptr(), state.q.data_ptr(), None, state.el.data_ptr(), rho.data_ptr(),
+        None, 0, C.byref(st), C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    return int(st.pair_count)
+
+
+def timing_read(m, cat, reset=True):
+    from pyrticle_b200 import _lib
+    ms = C.c_double()
+    k = C.c_int64()
+    _lib.check(m.lib.prt_workspace_timing_read(m.workspace, cat, C.byref(ms), C.byref(k),
+                                               int(reset)))
+    return ms.value, k.value
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def fp64_peak_tflops(torch):
+    """FP64 peak measured here: cuBLAS DGEMM 8192^3, best of 5 (CUDA events)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e9
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_baseline(w, target_seconds, threads=0, steps=1, seed=7):
+    """The oracle's multi-core path on a bounded random sample of the
+    workload's particles (full mesh and fields): particle-steps/s."""
+    from oracle import pyoracle as O
+    from pyrticle_b200 import meshgen, refelement
+    from pyrticle_b200.cloud import LSRK4_A, LSRK4_B
+    from pyrticle_b200.tools import PolynomialShapeFunction
+    from pyrticle_b200.units import SIUnitsWithNaturalConstants as U
+    om = O.OracleMesh(w.mesh, w.nodes, meshgen.element_bins(w.mesh))
+    ex = refelement.node_tuples(w.order)
+    pu = O.OraclePusher(ex, refelement.monomial_vandermonde(refelement.unit_nodes(w.order), ex),
+                        parallel=True)
+    sf = PolynomialShapeFunction(w.shape_radius, 3, 2)
+    c = U.VACUUM_LIGHT_SPEED()
+    rng = np.random.default_rng(seed)
+    threads = threads or O.max_threads()
+
+    def run(n):
+        idx = np.sort(rng.choice(w.particle_count, size=n, replace=False))
+        x, p = w.positions[idx], w.momenta[idx]
+        el = O.find_containing_elements(om, x, linear=False)
+        t0 = time.perf_counter()
+        r = O.pic_steps_parallel(pu, om, x, p, w.charges[idx], w.masses[idx], el,
+                                 list(w.fields), LSRK4_A, LSRK4_B, w.dt, c, steps, sf,
+                                 threads=threads)
+        dt = time.perf_counter() - t0
+        assert r["rc"] == 0
+        return dt
+
+    n = 200
+    dt = run(n)
+    per = dt / n
+    n = int(max(200, min(w.particle_count, target_seconds / max(per, 1e-9))))
+    dt = run(n)
+    return {"value": n * steps / dt, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{n} random particles of the workload x {steps} step(s) on the full "
+                      f"mesh/fields, oracle OpenMP build ({dt:.1f} s)"}
+
+
+def run_reference(args):
+    """The reference's CPU algorithms (restated in the oracle; the reference
+    itself cannot be built here) on the host cores, bounded sample per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from pyrticle_b200 import problems
+    w = problems.make(args.workload, scale=args.scale)
+    from oracle import pyoracle as O
+    threads = O.max_threads()
+    # one pilot to size the per-step sample to ~target seconds
+    per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    base = cpu_baseline(w, per_step, threads=threads)
+    n_per_step = int(base["value"] * per_step)
+    times = []
+    for k in range(args.warmup + args.steps):
+        b = cpu_baseline(w, per_step, threads=threads, seed=100 + k)
+        if k >= args.warmup:
+            times.append(b["value"])
+    value = float(np.mean(times))
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "particles_per_step_sample": n_per_step},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+                             "sample": base["sample"]},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    from pyrticle_b200 import _lib, problems
+
+    w = problems.make(args.workload, scale=args.scale, seed=1 + rank)
+    m, sf = build_method(w, torch)
+    s = m.make_state()
+    m.add_particles_from_arrays(s, w.positions, w.momenta, w.charges, w.masses)
+    fields = torch.as_tensor(w.fields, device="cuda")
+    n = len(s)
+    nn = len(m.discretization)
+
+    def one_step():
+        rho, j = m.step(s, fields, w.dt, steps=1, check=False)
+        if world > 1:
+            dist.all_reduce(rho)
+            dist.all_reduce(j)
+        return rho, j
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    pairs = count_pairs(m, s, sf)
+
+    # ---- timed region (device events, max over ranks) ----
+    clocks = ClockSampler(local)
+    _lib.check(m.lib.prt_workspace_timing(m.workspace, 1))
+    for cat in range(4):
+        timing_read(m, cat, reset=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        one_step()
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    _lib.check(m.lib.prt_workspace_timing(m.workspace, 0))
+    ms = e0.elapsed_time(e1)
+    kernel = {name: timing_read(m, cat) for cat, name in
+              enumerate(("deposit_gather", "deposit_stage", "lsrk_stage", "sort"))}
+    m.check_status()
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    value = world * n * args.steps / (ms * 1e-3)
+
+    # ---- end to end: host buffers through the same API ----
+    e2e = None
+    if not args.no_e2e:
+        hx = torch.empty_like(s.x, device="cpu").pin_memory()
+        hp = torch.empty_like(s.p, device="cpu").pin_memory()
+        hq = torch.empty_like(s.q, device="cpu").pin_memory()
+        hm = torch.empty_like(s.m, device="cpu").pin_memory()
+        he = torch.empty_like(s.el, device="cpu").pin_memory()
+        hx.copy_(s.x)
+        hp.copy_(s.p)
+        hq.copy_(s.q)
+        hm.copy_(s.m)
+        he.copy_(s.el)
+        hrho = torch.empty((nn,), dtype=torch.float64).pin_memory()
+        hj = torch.empty((3, nn), dtype=torch.float64).pin_memory()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for _ in range(args.steps):
+            s.x.copy_(hx, non_blocking=True)
+            s.p.copy_(hp, non_blocking=True)
+            s.q.copy_(hq, non_blocking=True)
+            s.m.copy_(hm, non_blocking=True)
+            s.el.copy_(he, non_blocking=True)
+            rho, j = one_step()
+            hrho.copy_(rho, non_blocking=True)
+            hj.copy_(j, non_blocking=True)
+        f1.record()
+        torch.cuda.synchronize()
+        ems = f0.elapsed_time(f1)
+        t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+        e2e = {"value": world * n * args.steps / (ems * 1e-3), "unit": METRIC,
+               "h2d_bytes_per_step": int(n * (24 + 24 + 8 + 8 + 4)),
+               "d2h_bytes_per_step": int(nn * 4 * 8)}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    peaks, src = measured_peaks()
+    fp64 = fp64_peak_tflops(torch)
+    gms, gk = kernel["deposit_gather"]
+    avg_gather = gms / max(gk, 1)
+    flops_per_launch = 15.0 * pairs
+    achieved = flops_per_launch / (avg_gather * 1e-3) / 1e12
+    sms, sk = kernel["lsrk_stage"]
+    stage_bytes = 216.0 * n
+    stage_gbs = stage_bytes / (sms / max(sk, 1) * 1e-3) / 1e9
+    roofline = {"bound": "fp64", "kernel": "gather_kernel<MeshTarget> (deposition)",
+                "achieved": achieved, "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
+                "traffic": None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 pipe; "
+                               "MEASURED_PEAKS.json has no FP64 figure)",
+                "algorithmic": f"15 flops x {pairs} (particle,node) pairs within the radius "
+                               f"per launch; {avg_gather:.3f} ms per launch",
+                "secondary": {"bound": "hbm", "kernel": "lsrk_stage_kernel<3>",
+                              "achieved": stage_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                              "frac": stage_gbs / peaks["hbm_gbs"],
+                              "algorithmic": "216 B per particle per stage",
+                              "peak_source": src}}
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded mesh, particles and fields of the workload)",
+            "config": {"workload": f"{args.workload}: {w.mesh.element_count} tets order "
+                                   f"{w.order}, {n} particles/GPU, shape radius "
+                                   f"{w.shape_radius * 100:g} cm, FP64 plain form",
+                       "particles_per_gpu": n, "elements": w.mesh.element_count,
+                       "nodes": nn, "order": w.order, "form": "fp64",
+                       "l2": "inputs larger than L2 (3.5 GB particle state per stage)",
+                       "parallelism": f"particles sharded over {world} GPU(s), NCCL "
+                                      "all-reduce of rho/j" if world > 1 else "1 GPU"},
+            "clocks": clk, "gpu_launches": None, "roofline": roofline,
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kernel.items()},
+            "pairs_per_deposition": pairs}
+    # libprt's own kernels in the timed region (CUB's radix-sort kernels not
+    # counted): per sort iota + 7 permutation gathers; per RK stage one fused
+    # kernel; per deposition bin keys, bin starts, payload and the gather.
+    line["gpu_launches"] = int(kernel["lsrk_stage"][1] + kernel["deposit_gather"][1] +
+                               3 * kernel["deposit_stage"][1] + 8 * kernel["sort"][1])
+    if e2e:
+        line["e2e"] = e2e
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

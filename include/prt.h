@@ -1,0 +1,320 @@
+/*
+ * prt.h -- C ABI of libprt.so, the B200 particle side of a pyrticle PIC step.
+ *
+ * The reference exposes this path through one Boost.Python module,
+ * pyrticle._internal (src/wrapper/wrap_main.cpp:43-57). Each entry point below
+ * names the reference interface it replaces. Conventions:
+ *
+ *   - every function returns int: PRT_OK (0) or a negative prt_status;
+ *   - particle vectors are device pointers in SoA layout: a 3-vector array is
+ *     [3][n] (component c of particle i at c*n + i); scalars are [n];
+ *   - node vectors are device pointers: rho [Nn], j [3][Nn] (the [vdim, Nn]
+ *     C-order layout PicMethod.deposit_j returns, pyrticle/cloud.py:535-538);
+ *   - element e owns nodes [e*Np, (e+1)*Np) (push_monomial.hpp:104-110);
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy stream);
+ *   - errors found on the device (the reference throws or warns there) are
+ *     recorded in the workspace status word and read by prt_workspace_status.
+ *
+ * No function here allocates device memory per call except the ones that
+ * take a prt_workspace, which grows its own scratch on demand.
+ */
+#ifndef PRT_H_INCLUDED
+#define PRT_H_INCLUDED
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PRT_INVALID_ELEMENT 0xffffffffu /* hedge::INVALID_ELEMENT */
+#define PRT_INVALID_AXIS 0xffffffffu    /* mesh_data::INVALID_AXIS, meshdata.hpp:68 */
+
+enum prt_status {
+  PRT_OK = 0,
+  PRT_ERR_INVALID_ARGUMENT = -1,
+  PRT_ERR_CUDA = -2,
+  PRT_ERR_OUT_OF_MEMORY = -3,
+  /* "no best normal found--weird" (particle_state.hpp:176-189) */
+  PRT_ERR_NO_BEST_NORMAL = -4,
+  /* a particle handed to a kernel has no containing element */
+  PRT_ERR_NOT_LOCATED = -5,
+  /* scratch larger than a fixed-capacity entry point supports */
+  PRT_ERR_CAPACITY = -6
+};
+
+/* Warnings recorded in the status word (the reference WARNs, tools.hpp:467-508). */
+enum prt_warning {
+  PRT_WARN_NONE = 0,
+  /* "deposited particle mass is zero" (dep_normshape.hpp:179-185) */
+  PRT_WARN_ZERO_MASS = 1
+};
+
+/* ---------------------------------------------------------------- mesh --- */
+
+/* Host-side description of mesh_data (meshdata.hpp:53-124), as filled by
+ * MeshData.fill_from_hedge (pyrticle/meshdata.py:37-133). All pointers are
+ * HOST pointers; prt_mesh_create copies them to the device. */
+typedef struct prt_mesh_desc {
+  int64_t element_count;            /* E */
+  int64_t vertex_count;             /* V */
+  int32_t nodes_per_element;        /* Np */
+  int32_t reserved0;
+  const double *vertices;           /* [V][3] */
+  const uint32_t *element_vertices; /* [E][4] */
+  const double *inverse_maps;       /* [E][12]: row-major A (3x3), then b (3) */
+  const double *jacobians;          /* [E] |det| of the unit->element map */
+  const double *face_normals;       /* [E][4][3] outward unit normals */
+  const double *face_plane_rhs;     /* [E][4] n . x on the face */
+  const double *face_centroids;     /* [E][4][3] */
+  const double *face_radii;         /* [E][4] bounding-circle radius */
+  const uint32_t *face_neighbors;   /* [E][4] or PRT_INVALID_ELEMENT */
+  const uint32_t *face_periodicity_axes; /* [E][4] or PRT_INVALID_AXIS */
+  const uint32_t *vertex_adj_starts;     /* [V+1] */
+  const uint32_t *vertex_adj_elements;   /* ascending element id per vertex */
+  double periodicity_min[3];        /* min == max: axis not periodic */
+  double periodicity_max[3];
+  const double *nodes;              /* [E*Np][3] node coordinates */
+  /* element bins for the global search (meshdata.hpp:208-215): bin b lists,
+   * ascending, every element whose bounding box overlaps it */
+  double bin_origin[3];
+  double bin_inv_width[3];
+  int32_t bin_dims[3];
+  int32_t reserved1;
+  const uint32_t *bin_starts;       /* [bins+1] */
+  const uint32_t *bin_elements;
+} prt_mesh_desc;
+
+typedef struct prt_mesh prt_mesh;
+
+/* Replaces MeshData(dim) + fill_from_hedge (wrap_meshdata.cpp:50-114). */
+int prt_mesh_create(const prt_mesh_desc *desc, prt_mesh **out);
+int prt_mesh_destroy(prt_mesh *mesh);
+
+/* ----------------------------------------------------------- workspace --- */
+
+typedef struct prt_workspace prt_workspace;
+
+int prt_workspace_create(prt_workspace **out);
+int prt_workspace_destroy(prt_workspace *ws);
+/* Synchronises `stream`, returns the first recorded device error (or PRT_OK)
+ * with the particle index that raised it, and the first warning; clears both
+ * when `clear` is nonzero. */
+int prt_workspace_status(prt_workspace *ws, void *stream, int32_t *error,
+                         int64_t *error_index, int32_t *warning,
+                         int64_t *warning_index, int32_t clear);
+
+/* Find-path event counters (particle_state.hpp:86-92, cloud.py:366-377). */
+typedef struct prt_find_counters {
+  uint64_t find_same;
+  uint64_t find_by_neighbor;
+  uint64_t find_by_vertex;
+  uint64_t find_global;
+} prt_find_counters;
+
+/* Copies the workspace's device counters to *out (synchronising `stream`)
+ * and zeroes them when `reset` is nonzero. */
+int prt_workspace_counters(prt_workspace *ws, void *stream,
+                           prt_find_counters *out, int32_t reset);
+
+/* Kernel timing (measurement hook; no reference counterpart). When enabled,
+ * the library brackets its main kernels with CUDA events on the launch
+ * stream; prt_workspace_timing_read sums the elapsed times per category
+ * (synchronising) and optionally resets them. */
+enum prt_timing_category {
+  PRT_TIME_DEPOSIT_GATHER = 0, /* node-centric deposition kernel */
+  PRT_TIME_DEPOSIT_STAGE = 1,  /* particle binning, sort and packing */
+  PRT_TIME_LSRK_STAGE = 2,     /* fused RK stage kernel */
+  PRT_TIME_SORT = 3,           /* prt_sort_by_element */
+  PRT_TIME_CATEGORIES = 4
+};
+int prt_workspace_timing(prt_workspace *ws, int32_t enable);
+int prt_workspace_timing_read(prt_workspace *ws, int32_t category,
+                              double *total_ms, int64_t *launches,
+                              int32_t reset);
+
+/* ---------------------------------------------------------- kinematics --- */
+
+/* Replaces get_velocities(ps, c) (particle_state.hpp:98-125,
+ * wrap_pic.cpp:71): v = c p / sqrt(m^2 c^2 + |p|^2), zero for p = 0. */
+int prt_get_velocities(int64_t n, const double *momenta, const double *masses,
+                       double vacuum_c, double *velocities, void *stream);
+
+/* Replaces MeshData.find_containing_element(pt) (meshdata.hpp:208-215) used by
+ * PicMethod.add_particles (cloud.py:470): the lowest-id element whose inverse
+ * map passes is_in_unit_simplex, or PRT_INVALID_ELEMENT. */
+int prt_find_containing_elements(const prt_mesh *mesh, int64_t n,
+                                 const double *positions, uint32_t *elements,
+                                 void *stream);
+
+/* Replaces update_containing_elements(mesh, ps, bhit_listener, counters)
+ * (particle_state.hpp:266-357, wrap_pic.cpp:73). A particle that is found
+ * nowhere, even after the periodic wrap, gets PRT_INVALID_ELEMENT: the
+ * caller removes it (the reference kills it through the boundary-hit
+ * listener, cloud.py:581-585). Particles that already carry
+ * PRT_INVALID_ELEMENT are skipped. Counters accumulate in `ws`. */
+int prt_update_containing_elements(const prt_mesh *mesh, prt_workspace *ws,
+                                   int64_t n, double *positions,
+                                   const double *momenta, uint32_t *elements,
+                                   void *stream);
+
+/* ------------------------------------------------------ monomial pusher --- */
+
+typedef struct prt_pusher prt_pusher;
+
+/* Replaces MonomialPusher3d3v(mesh) + LocalMonomialDiscretization set-up
+ * (pusher.py:86-114, push_monomial.hpp:45-80): `exponents` [Np][3] are the
+ * monomial exponents, `vandermonde` [Np][Np] row-major is V[i][k] =
+ * monomial_k(unit_node_i). */
+int prt_monomial_pusher_create(const prt_mesh *mesh, int32_t np,
+                               const uint32_t *exponents,
+                               const double *vandermonde, prt_pusher **out);
+int prt_monomial_pusher_destroy(prt_pusher *pusher);
+
+/* Replaces MonomialPusher3d3v.forces(ex, ey, ez, bx, by, bz, ps, velocities,
+ * vis_listener) (push_monomial.hpp:219-325, wrap_pusher.cpp:160-165):
+ * forces[3][n] = q E(x) + v x (q B(x)). fields[k] is a device [Nn] array or
+ * NULL for a zero component. vis, if not NULL, receives [4][3][n]: pt_e, pt_b,
+ * el_force, mag_force (the verbose_vis vectors, push_monomial.hpp:307-322).
+ * Particles with element PRT_INVALID_ELEMENT get zero force. */
+int prt_forces(const prt_pusher *pusher, int64_t n, const double *positions,
+               const uint32_t *elements, const double *charges,
+               const double *velocities, const double *const fields[6],
+               double *forces, double *vis, void *stream);
+
+/* One low-storage Runge-Kutta stage of the particle ODE, fused:
+ *   f = (v(p), F(x, p)),  k = a k + dt f,  (x, p) += b k,  relocate.
+ * This is PicMethod.advance_state (cloud.py:554-603) driven by the 2N-storage
+ * RK update through TimesteppablePicState.__add__ (cloud.py:172-186), with the
+ * force of prt_forces and the relocation of prt_update_containing_elements.
+ * kx, kp are the [3][n] residuals; dead particles (PRT_INVALID_ELEMENT) are
+ * left untouched. `precision` 0 = FP64 plain form. */
+int prt_lsrk_stage(const prt_pusher *pusher, prt_workspace *ws, int64_t n,
+                   double *positions, double *momenta, const double *charges,
+                   const double *masses, uint32_t *elements, double *kx,
+                   double *kp, const double *const fields[6], double rk_a,
+                   double rk_b, double dt, double vacuum_c, int32_t precision,
+                   void *stream);
+
+/* ----------------------------------------------------------- deposition --- */
+
+/* polynomial_shape_function(radius, dimensions, alpha) (tools.hpp:514-556,
+ * tools.cpp:43-58): S(r) = normalizer * (radius - r^2/radius)^alpha inside
+ * the radius, 0 outside. */
+typedef struct prt_shape_function {
+  double radius;
+  double alpha;
+  double normalizer;
+} prt_shape_function;
+
+enum prt_deposit_mode {
+  PRT_DEPOSIT_PLAIN = 0,      /* ShapeFunctionDepositor (dep_shape.hpp) */
+  PRT_DEPOSIT_NORMALIZED = 1  /* NormalizedShapeFunctionDepositor (dep_normshape.hpp) */
+};
+
+/* Per-call statistics of the normalising depositor (dep_normshape.hpp:42-47):
+ * count / sum / sum of squares / min / max of the applied scale q / integral
+ * and of the number of elements each particle reaches. */
+typedef struct prt_deposit_stats {
+  double norm_count, norm_sum, norm_sum_sq, norm_min, norm_max;
+  double el_count, el_sum, el_sum_sq, el_min, el_max;
+  /* number of (particle, node) pairs with |x_node - x_p| <= radius */
+  double pair_count;
+} prt_deposit_stats;
+
+/* Replaces deposit_rho / deposit_j / deposit_densities(dep, ds, ps,
+ * node_count, [velocities,] slice) for InterpolatingDepositor3d3v and
+ * NormalizingInterpolatingDepositor3d3v (dep_target.hpp:203-273,
+ * wrap_depositor.cpp:44-50):
+ *   rho[n]    = sum_p w_p S(x_n - x_p),  j[c][n] = sum_p w_p v_p[c] S(x_n - x_p)
+ * with w_p = q_p (plain) or q_p / (sum_e |J_e| sum_i w_i S(x_i - x_p))
+ * (normalised, `integral_weights` [Np] = M 1). rho or j may be NULL. The sum
+ * is deterministic: no floating-point atomics, fixed order.
+ * Particles with element PRT_INVALID_ELEMENT are skipped. When `stats` is
+ * not NULL the call also counts the (particle, node) pairs inside the
+ * radius, and synchronises `stream`. */
+int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
+                      prt_shape_function shape, const double *integral_weights,
+                      int64_t n, const double *positions, const double *charges,
+                      const double *velocities, const uint32_t *elements,
+                      double *rho, double *j, int32_t precision,
+                      prt_deposit_stats *stats, void *stream);
+
+/* ------------------------------------------------------------ grid dep --- */
+
+/* One brick (grid.hpp:159-340): cell-centred points origin + (idx + 1/2) h,
+ * global index start_index + idx . strides with x fastest. */
+typedef struct prt_brick {
+  double origin[3];
+  double stepwidths[3];
+  int32_t dims[3];
+  int32_t reserved;
+  int64_t start_index;
+} prt_brick;
+
+enum prt_grid_weights {
+  PRT_GRID_SHAPE = 0,     /* q S(x - pt) at brick points (dep_grid.hpp:220-264) */
+  PRT_GRID_TRILINEAR = 1  /* q * trilinear weights on the 8 surrounding points */
+};
+
+typedef struct prt_grid prt_grid;
+
+/* Replaces RegularGridDepositor3d3v(mesh) with .bricks and .elements_on_grid
+ * filled (wrap_depositor.cpp:66-102, grid.py:71-117): per element-on-grid,
+ * its element number, grid node list, weight factors and the Np x |G|
+ * column-major interpolation matrix. Average groups (dep_grid.hpp:108-117) are
+ * given as CSR; avg_group_count = 0 disables continuity enforcement. */
+typedef struct prt_grid_desc {
+  int32_t brick_count;
+  int32_t nodes_per_element;
+  const prt_brick *bricks;
+  int64_t eog_count;
+  const uint32_t *eog_elements;     /* [eog_count] */
+  const uint64_t *eog_starts;       /* [eog_count+1] offsets into nodes/weights */
+  const uint32_t *eog_grid_nodes;   /* [total] */
+  const double *eog_weights;        /* [total] */
+  const uint64_t *eog_matrix_starts;/* [eog_count+1] offsets into matrices */
+  const double *eog_matrices;       /* column-major Np x |G_e| each */
+  int64_t avg_group_count;
+  const uint32_t *avg_group_starts; /* [avg_group_count+1] */
+  const uint32_t *avg_group_nodes;
+} prt_grid_desc;
+
+int prt_grid_create(const prt_mesh *mesh, const prt_grid_desc *desc,
+                    prt_grid **out);
+int prt_grid_destroy(prt_grid *grid);
+
+/* Replaces deposit_grid_rho / deposit_grid_j / deposit_grid_densities
+ * (dep_grid.hpp:441-501) including periodic copies (dep_grid_base.hpp:285-347).
+ * grid_rho [G] and grid_j [3][G] (either may be NULL). Deterministic. */
+int prt_deposit_grid(const prt_grid *grid, prt_workspace *ws, int32_t weights,
+                     prt_shape_function shape, int64_t n,
+                     const double *positions, const double *charges,
+                     const double *velocities, const uint32_t *elements,
+                     double *grid_rho, double *grid_j, void *stream);
+
+/* Replaces remap_grid_to_mesh(from, to, offset, increment)
+ * (dep_grid.hpp:270-358): for every element-on-grid,
+ * to[(start + i)*increment + offset] += sum_k I[i,k] w_k from[offset + g_k*increment]
+ * followed by the average-group continuity pass. `to` is accumulated into. */
+int prt_remap_grid_to_mesh(const prt_grid *grid, const double *from,
+                           double *to, int64_t offset, int64_t increment,
+                           void *stream);
+
+/* ---------------------------------------------------------------- misc --- */
+
+/* Sorts the particle store by containing element (stable), permuting every
+ * given [n] / [3][n] array in place through `ws` scratch. Arrays may be NULL. */
+int prt_sort_by_element(prt_workspace *ws, int64_t n, uint32_t *elements,
+                        double *positions, double *momenta, double *charges,
+                        double *masses, double *kx, double *kp, int64_t *ids,
+                        void *stream);
+
+/* Library version string. */
+const char *prt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PRT_H_INCLUDED */

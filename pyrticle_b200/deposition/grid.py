@@ -1,0 +1,348 @@
+"""Grid depositor: deposit onto brick grids, then remap element by element
+onto the DG nodes (the reference's ``deposition/grid.py``, ``dep_grid.hpp``,
+``dep_grid_base.hpp`` and ``grid.hpp``).
+
+Set-up (host, numpy, batched over elements) follows the reference's
+``prepare_with_pointwise_projection_and_basis_reduction`` (grid.py:552-669):
+per element, the grid points inside the element (grown by ``el_tolerance``
+times the norm of the element map, dep_grid.hpp:142-213) weighted by
+sqrt(cell volume), the weighted orthonormal Vandermonde on them, and a
+basis reduction that drops the highest-degree mode with the largest weight
+in the last right singular vector while the system is underdetermined or its
+condition number exceeds 10. The remap matrix is
+``I_e = V_e[:, basis] pinv(W V_struct[:, basis])`` (grid.py:217-273).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from .. import _lib, refelement
+from . import Depositor
+from .grid_base import SingleBrickGenerator
+
+
+class BrickInfo:
+    """One brick (grid.hpp:159-340): cell-centred points, x-fastest numbering."""
+
+    def __init__(self, number, start_index, stepwidths, origin, dims):
+        stepwidths = np.array(stepwidths, dtype=np.float64)
+        origin = np.array(origin, dtype=np.float64)
+        dims = np.array(dims, dtype=np.int64)
+        neg = stepwidths < 0
+        stepwidths[neg] *= -1
+        origin[neg] -= stepwidths[neg] * dims[neg]
+        if (dims <= 0).any():
+            raise ValueError("zero dimensions for brick not supported")
+        self.number = number
+        self.start_index = int(start_index)
+        self.stepwidths = stepwidths
+        self.origin = origin
+        self.dims = dims
+        self.strides = np.array([1, dims[0], dims[0] * dims[1]], dtype=np.int64)
+
+    def __len__(self):
+        return int(np.prod(self.dims))
+
+    def node_count(self):
+        return len(self)
+
+    def cell_volume(self):
+        return float(np.prod(self.stepwidths))
+
+    def bounding_box(self):
+        return self.origin, self.origin + self.dims * self.stepwidths
+
+    def point(self, idx):
+        return self.origin + self.stepwidths / 2 + np.asarray(idx) * self.stepwidths
+
+    def index(self, idx):
+        return self.start_index + int(np.dot(idx, self.strides))
+
+    def as_struct(self) -> _lib.Brick:
+        b = _lib.Brick()
+        for a in range(3):
+            b.origin[a] = self.origin[a]
+            b.stepwidths[a] = self.stepwidths[a]
+            b.dims[a] = int(self.dims[a])
+        b.start_index = self.start_index
+        return b
+
+
+def find_points_in_elements(mesh, bricks, el_tolerance, chunk=20000):
+    """Per element, the grid points within the tolerance-grown element
+    (dep_grid.hpp:142-213). Returns (starts[E+1], grid_index, points, weights)."""
+    E = mesh.element_count
+    A = mesh.forward_maps[:, :9].reshape(E, 3, 3)
+    scaled_tol = el_tolerance * np.linalg.norm(A, ord=2, axis=(1, 2))
+    p = mesh.points[mesh.elements]
+    elo = p.min(axis=1) - scaled_tol[:, None]
+    ehi = p.max(axis=1) + scaled_tol[:, None]
+    per_el_idx = [[] for _ in range(E)]
+    per_el_pts = [[] for _ in range(E)]
+    per_el_w = [[] for _ in range(E)]
+    counts = np.zeros(E, dtype=np.int64)
+    all_idx, all_pts, all_w, all_el = [], [], [], []
+    for brk in bricks:
+        blo, bhi = brk.bounding_box()
+        dV = brk.cell_volume()
+        ilo_box = np.maximum(elo, blo)
+        ihi_box = np.minimum(ehi, bhi)
+        nonempty = np.all(ilo_box < ihi_box, axis=1)
+        lo_i = np.floor((ilo_box - brk.origin) / brk.stepwidths).astype(np.int64)
+        hi_i = np.ceil((ihi_box - brk.origin) / brk.stepwidths).astype(np.int64)
+        ext = np.where(nonempty[:, None], np.maximum(hi_i - lo_i, 0), 0)
+        mx = ext.max(axis=0)
+        for c0 in range(0, E, chunk):
+            sl = slice(c0, min(E, c0 + chunk))
+            ee = np.arange(sl.start, sl.stop)
+            ox, oy, oz = np.meshgrid(np.arange(mx[0]), np.arange(mx[1]), np.arange(mx[2]),
+                                     indexing="ij")
+            # x fastest, like the brick iterator (grid.hpp:104-125)
+            off = np.stack([ox.transpose(2, 1, 0).ravel(), oy.transpose(2, 1, 0).ravel(),
+                            oz.transpose(2, 1, 0).ravel()], axis=1)      # [K, 3]
+            idx = lo_i[sl][:, None, :] + off[None]                          # [e, K, 3]
+            valid = np.all(off[None] < ext[sl][:, None, :], axis=2)
+            pts = brk.origin + brk.stepwidths / 2 + idx * brk.stepwidths   # [e, K, 3]
+            n = mesh.face_normals[sl]                                       # [e, 4, 3]
+            rhs = mesh.face_plane_rhs[sl]
+            dist = np.einsum("eki,efi->ekf", pts, n) - rhs[:, None, :]
+            inside = valid & np.all(dist <= scaled_tol[sl][:, None, None], axis=2)
+            e_i, k_i = np.nonzero(inside)                                   # row-major
+            gidx = brk.start_index + idx[e_i, k_i] @ brk.strides
+            all_el.append(ee[e_i])
+            all_idx.append(gidx)
+            all_pts.append(pts[e_i, k_i])
+            all_w.append(np.full(len(e_i), np.sqrt(dV)))
+    el = np.concatenate(all_el)
+    order = np.argsort(el, kind="stable")   # bricks in order, points in iterator order
+    el = el[order]
+    gidx = np.concatenate(all_idx)[order]
+    pts = np.concatenate(all_pts)[order]
+    w = np.concatenate(all_w)[order]
+    starts = np.zeros(E + 1, dtype=np.int64)
+    starts[1:] = np.cumsum(np.bincount(el, minlength=E))
+    return starts, gidx, pts, w
+
+
+def basis_reduction_matrices(mesh, order, starts, pts, w, max_condition=10.0):
+    """Batched basis reduction + pseudoinverse (grid.py:217-273, 552-669).
+
+    Returns per element the column-major Np x P_e interpolation matrix
+    (flattened, concatenated) and the kept-mode count."""
+    E = mesh.element_count
+    modes = refelement.mode_identifiers(order)
+    Np = len(modes)
+    degree = np.array([sum(m) for m in modes])
+    el_vdm = refelement.orthonormal_vandermonde(refelement.unit_nodes(order), modes)
+    A_inv = mesh.inverse_maps[:, :9].reshape(E, 3, 3)
+    b_inv = mesh.inverse_maps[:, 9:]
+    counts = np.diff(starts)
+    el_of_pt = np.repeat(np.arange(E), counts)
+    unit = np.einsum("pij,pj->pi", A_inv[el_of_pt], pts) + b_inv[el_of_pt]
+    vfull = orthonormal_vandermonde_fast(unit, modes) * w[:, None]       # [Ptot, Np]
+    mats = [None] * E
+    kept = np.zeros(E, dtype=np.int64)
+    eps = np.finfo(float).eps
+    for P in np.unique(counts):
+        els = np.nonzero(counts == P)[0]
+        if P == 0:
+            raise RuntimeError("grid depositor: element %d contains no grid points" % els[0])
+        rows = starts[els][:, None] + np.arange(P)[None]                    # [G, P]
+        V = vfull[rows]                                                    # [G, P, Np]
+        mask = np.ones((len(els), Np), dtype=bool)
+        active = np.arange(len(els))
+        B = Np
+        while len(active):
+            cols = np.nonzero(mask[active])[1].reshape(len(active), B)
+            Vs = np.take_along_axis(V[active], cols[:, None, :], axis=2)  # [g, P, B]
+            u, s, vt = _batched_svd(Vs)
+            ratio = np.abs(s[:, 0] / s[:, -1]) if s.shape[1] else np.full(len(active), np.inf)
+            retry = (B > P) | ~(ratio <= max_condition)
+            done = active[~retry]
+            if len(done):
+                g = ~retry
+                ss = s[g]
+                thresh = eps * max(P, B) * ss[:, :1]
+                inv_s = np.where(np.abs(ss) >= thresh, 1.0 / np.where(ss == 0, 1, ss), 0.0)
+                k = ss.shape[1]
+                inv_diag = np.zeros((len(done), B, P))
+                inv_diag[:, np.arange(k), np.arange(k)] = inv_s
+                pinv = np.transpose(vt[g], (0, 2, 1)) @ inv_diag @ np.transpose(u[g], (0, 2, 1))
+                ev = el_vdm[:, cols[g]].transpose(1, 0, 2)                  # [d, Np, B]
+                imat = ev @ pinv                                            # [d, Np, P]
+                for t, gi in enumerate(done):
+                    e = els[gi]
+                    mats[e] = np.asfortranarray(imat[t]).ravel(order="F")
+                    kept[e] = B
+            if not retry.any():
+                break
+            if B == 1:
+                raise RuntimeError("basis reduction has killed almost the entire basis on "
+                                   "element %d" % els[active[retry][0]])
+            ra = active[retry]
+            vti = vt[retry][:, -1, :]                                       # [r, B]
+            deg = degree[cols[retry]]                                       # [r, B]
+            killable = deg == deg.max(axis=1, keepdims=True)
+            score = np.where(killable, np.abs(vti), -1.0)
+            kill_pos = np.argmax(score, axis=1)                             # first max
+            kill_col = cols[retry][np.arange(len(ra)), kill_pos]
+            mask[ra, kill_col] = False
+            active = ra
+            B -= 1
+    mstarts = np.zeros(E + 1, dtype=np.int64)
+    mstarts[1:] = np.cumsum(counts * Np)
+    return np.concatenate(mats), mstarts, kept
+
+
+def _batched_svd(A):
+    try:
+        return np.linalg.svd(A, full_matrices=True)
+    except np.linalg.LinAlgError:
+        outs = [np.linalg.svd(a, full_matrices=True) for a in A]
+        return (np.stack([o[0] for o in outs]), np.stack([o[1] for o in outs]),
+                np.stack([o[2] for o in outs]))
+
+
+def orthonormal_vandermonde_fast(points, modes):
+    return refelement.orthonormal_vandermonde(points, modes)
+
+
+class GridDepositor(Depositor):
+    """Deposit on brick grids (shape-function values at the points, or
+    trilinear weights with ``grid_weights="trilinear"``), then remap."""
+
+    def __init__(self, brick_generator=None, el_tolerance=0.12, max_extra_points=20,
+                 enforce_continuity=False, submethod="simplex_reduce",
+                 filter_min_amplification=None, filter_order=None, jiggle_radius=0.0,
+                 grid_weights="shape"):
+        Depositor.__init__(self)
+        self.brick_generator = brick_generator or SingleBrickGenerator()
+        self.el_tolerance = el_tolerance
+        self.max_extra_points = max_extra_points
+        self.enforce_continuity = enforce_continuity
+        self.submethod = submethod
+        if submethod != "simplex_reduce":
+            raise NotImplementedError("only submethod='simplex_reduce' (the reference default)")
+        if filter_min_amplification is not None or jiggle_radius:
+            raise NotImplementedError("filters and jiggly bricks are not supported")
+        if grid_weights not in ("shape", "trilinear"):
+            raise ValueError("grid_weights must be 'shape' or 'trilinear'")
+        self.grid_weights = grid_weights
+
+    @property
+    def name(self):
+        return "GridRegular"
+
+    def initialize(self, method):
+        Depositor.initialize(self, method)
+        discr = method.discretization
+        self.bricks = []
+        start = 0
+        for i, (sw, origin, dims) in enumerate(self.brick_generator(discr)):
+            b = BrickInfo(i, start, sw, origin, dims)
+            self.bricks.append(b)
+            start += len(b)
+        self.grid_node_count = start
+        starts, gidx, pts, w = find_points_in_elements(discr.mesh, self.bricks,
+                                                       self.el_tolerance)
+        mats, mstarts, kept = basis_reduction_matrices(discr.mesh, discr.order, starts, pts, w)
+        self.eog = dict(starts=starts, grid_nodes=gidx, weights=w, matrices=mats,
+                        matrix_starts=mstarts, kept=kept)
+        keep = []
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep.append(a)
+            return a
+
+        d = _lib.GridDesc()
+        d.brick_count = len(self.bricks)
+        d.nodes_per_element = discr.nodes_per_element
+        barr = (_lib.Brick * len(self.bricks))(*[b.as_struct() for b in self.bricks])
+        keep.append(barr)
+        d.bricks = C.cast(barr, C.POINTER(_lib.Brick))
+        E = discr.mesh.element_count
+        d.eog_count = E
+        d.eog_elements = _lib.ptr(arr(np.arange(E), np.uint32), C.c_uint32)
+        d.eog_starts = _lib.ptr(arr(starts, np.uint64), C.c_uint64)
+        d.eog_grid_nodes = _lib.ptr(arr(gidx, np.uint32), C.c_uint32)
+        d.eog_weights = _lib.ptr(arr(w, np.float64))
+        d.eog_matrix_starts = _lib.ptr(arr(mstarts, np.uint64), C.c_uint64)
+        d.eog_matrices = _lib.ptr(arr(mats, np.float64))
+        d.avg_group_count = 0
+        self.grid_desc = d
+        self._keep = keep
+        h = C.c_void_p()
+        _lib.check(self.lib.prt_grid_create(method.mesh_data.handle, C.byref(d), C.byref(h)),
+                   "prt_grid_create")
+        self.handle = h
+
+    def __del__(self):
+        if getattr(self, "handle", None) is not None and _lib._lib is not None:
+            _lib._lib.prt_grid_destroy(self.handle)
+            self.handle = None
+
+    def grid_node_count_with_extra(self):
+        return self.grid_node_count
+
+    def _shape_desc(self):
+        sf = self.shape_function
+        if sf is None:
+            return _lib.ShapeFunctionDesc(0.0, 2.0, 0.0)
+        return _lib.ShapeFunctionDesc(sf.radius, sf.exponent, sf.normalizer)
+
+    def deposit_grid_densities_device(self, state, rho=True, j=True):
+        if self.grid_weights == "shape":
+            self.deposit_hook()
+        m = self.method
+        G = self.grid_node_count
+        dev = state.x.device
+        gr = torch.empty((G,), dtype=torch.float64, device=dev) if rho else None
+        gj = torch.empty((3, G), dtype=torch.float64, device=dev) if j else None
+        v = m.velocities_device(state) if j else None
+        wmode = _lib.GRID_SHAPE if self.grid_weights == "shape" else _lib.GRID_TRILINEAR
+        _lib.check(self.lib.prt_deposit_grid(
+            self.handle, m.workspace, wmode, self._shape_desc(), len(state),
+            state.x.data_ptr(), state.q.data_ptr(), v.data_ptr() if v is not None else None,
+            state.el.data_ptr(), gr.data_ptr() if rho else None,
+            gj.data_ptr() if j else None, self._stream()), "prt_deposit_grid")
+        return gr, gj
+
+    def remap_grid_to_mesh_device(self, q_grid: torch.Tensor) -> torch.Tensor:
+        """[G] -> [Nn]; [3, G] -> [3, Nn] (each component remapped)."""
+        nn = len(self.method.discretization)
+        if q_grid.dim() == 1:
+            out = torch.zeros((nn,), dtype=torch.float64, device=q_grid.device)
+            _lib.check(self.lib.prt_remap_grid_to_mesh(self.handle, q_grid.data_ptr(),
+                                                       out.data_ptr(), 0, 1, self._stream()))
+            return out
+        out = torch.zeros((q_grid.shape[0], nn), dtype=torch.float64, device=q_grid.device)
+        for c in range(q_grid.shape[0]):
+            _lib.check(self.lib.prt_remap_grid_to_mesh(
+                self.handle, q_grid[c].contiguous().data_ptr(), out[c].data_ptr(), 0, 1,
+                self._stream()))
+        return out
+
+    def deposit_densities_device(self, state, rho=True, j=True):
+        gr, gj = self.deposit_grid_densities_device(state, rho, j)
+        r = self.remap_grid_to_mesh_device(gr) if rho else None
+        jj = self.remap_grid_to_mesh_device(gj) if j else None
+        return r, jj
+
+    # host entry points with the reference's names
+    def deposit_grid_rho(self, state, pslice=None):
+        return self.deposit_grid_densities_device(state, True, False)[0].cpu().numpy()
+
+    def deposit_grid_j(self, state, velocities=None, pslice=None):
+        return self.deposit_grid_densities_device(state, False, True)[1].T.contiguous().cpu().numpy()
+
+    def remap_grid_to_mesh(self, q_grid):
+        t = torch.as_tensor(np.ascontiguousarray(q_grid), device=self.method.dev)
+        if t.dim() == 2:
+            t = t.T.contiguous()
+            return self.remap_grid_to_mesh_device(t).T.contiguous().cpu().numpy()
+        return self.remap_grid_to_mesh_device(t).cpu().numpy()

@@ -1,0 +1,143 @@
+"""Shape functions, statistics and warnings (``tools.hpp``, ``tools.cpp``,
+``pyrticle/tools.py`` of the reference)."""
+
+from __future__ import annotations
+
+import math
+import warnings
+
+import numpy as np
+
+
+def sphere_area(dims: float) -> float:
+    """Surface area of the unit sphere in ``dims`` dimensions (tools.cpp:35-38)."""
+    return 2 * math.pi ** (dims / 2) / math.gamma(dims / 2)
+
+
+def _beta(a: float, b: float) -> float:
+    return math.exp(math.lgamma(a) + math.lgamma(b) - math.lgamma(a + b))
+
+
+class PolynomialShapeFunction:
+    """S(r) = N (a - r^2/a)^alpha for r <= a, else 0 (tools.hpp:514-556).
+
+    The normaliser ``N = 2 / (|S^{n-1}| a^{n+alpha} B(n/2, alpha+1))``
+    (tools.cpp:43-58) makes S integrate to one over R^n.
+    """
+
+    def __init__(self, radius: float = 1.0, dimensions: int = 1, alpha: float = 2.0):
+        self.radius = float(radius)
+        self.dimensions = int(dimensions)
+        self.exponent = float(alpha)
+        n = float(dimensions)
+        self.normalizer = 2 / (sphere_area(n) * self.radius ** (n + alpha)
+                               * _beta(n / 2, alpha + 1))
+
+    @property
+    def alpha(self) -> float:
+        return self.exponent
+
+    def __call__(self, r) -> float:
+        r = np.asarray(r, dtype=np.float64)
+        r2 = float(np.dot(r, r))
+        if r2 > self.radius ** 2:
+            return 0.0
+        t = self.radius - r2 / self.radius
+        return self.normalizer * t ** self.exponent
+
+    def evaluate(self, r: np.ndarray) -> np.ndarray:
+        """Vectorised over the last axis of ``r``."""
+        r2 = np.sum(np.asarray(r) ** 2, axis=-1)
+        t = np.maximum(self.radius - r2 / self.radius, 0.0)
+        out = self.normalizer * t ** self.exponent
+        out[r2 > self.radius ** 2] = 0.0
+        return out
+
+    @staticmethod
+    def name() -> str:
+        return "polynomial"
+
+
+class StatsGatherer:
+    """Welford mean/variance with min and max (tools.hpp:340-417)."""
+
+    def __init__(self):
+        self.reset()
+
+    def reset(self):
+        self._count = 0
+        self._mean = 0.0
+        self._m2 = 0.0
+        self._min = None
+        self._max = None
+
+    def add(self, x: float) -> None:
+        x = float(x)
+        if self._count == 0 or x < self._min:
+            self._min = x
+        if self._count == 0 or x > self._max:
+            self._max = x
+        self._count += 1
+        delta = x - self._mean
+        self._mean += delta / self._count
+        self._m2 += delta * (x - self._mean)
+
+    def add_moments(self, count, total, total_sq, lo, hi) -> None:
+        """Merge a block summarised by count / sum / sum of squares / min / max."""
+        count = int(count)
+        if count == 0:
+            return
+        mean_b = total / count
+        m2_b = max(total_sq - count * mean_b * mean_b, 0.0)
+        n = self._count + count
+        delta = mean_b - self._mean
+        self._m2 += m2_b + delta * delta * self._count * count / n
+        self._mean += delta * count / n
+        self._min = lo if self._min is None else min(self._min, lo)
+        self._max = hi if self._max is None else max(self._max, hi)
+        self._count = n
+
+    def count(self) -> int:
+        return self._count
+
+    def minimum(self):
+        return self._min
+
+    def maximum(self):
+        return self._max
+
+    def mean(self) -> float:
+        if self._count == 0:
+            raise RuntimeError("attempted to take empty mean")
+        return self._mean
+
+    def variance_sample(self) -> float:
+        if self._count < 2:
+            raise RuntimeError("sample too small for sample variance")
+        return self._m2 / (self._count - 1)
+
+    def standard_deviation_sample(self) -> float:
+        return math.sqrt(self.variance_sample())
+
+    def variance(self) -> float:
+        if self._count == 0:
+            raise RuntimeError("attempted to take empty variance")
+        return self._m2 / self._count
+
+    def standard_deviation(self) -> float:
+        return math.sqrt(self.variance())
+
+
+class WarningForwarder:
+    """Routes core warnings to Python's ``warnings`` (pyrticle/tools.py:31-46)."""
+
+    def note_warning(self, message, filename="libprt", lineno=0):
+        warnings.warn_explicit(message, UserWarning, filename, lineno)
+
+
+class WarningIgnorer:
+    def note_warning(self, message, filename="libprt", lineno=0):
+        pass
+
+
+warning_forwarder = WarningForwarder()

@@ -1,0 +1,110 @@
+"""Host-side set-up logic (no GPU): reference element, meshes, stats,
+grid-depositor remap matrices, LSRK4 coefficients."""
+
+import math
+
+import numpy as np
+import pytest
+
+from pyrticle_b200 import meshgen, problems, refelement
+from pyrticle_b200.cloud import LSRK4_A, LSRK4_B, LSRK4_C
+from pyrticle_b200.deposition.grid import (BrickInfo, basis_reduction_matrices,
+                                           find_points_in_elements)
+from pyrticle_b200.tools import StatsGatherer
+
+
+@pytest.mark.parametrize("order", [1, 2, 3, 4])
+def test_nodes_edges_are_gauss_lobatto(order):
+    n = refelement.unit_nodes(order)
+    assert len(n) == refelement.node_count(order)
+    e = np.sort(n[(np.abs(n[:, 1] + 1) < 1e-12) & (np.abs(n[:, 2] + 1) < 1e-12)][:, 0])
+    assert np.allclose(e, refelement.gauss_lobatto_nodes(order), atol=1e-14)
+    assert (n >= -1 - 1e-12).all() and (n.sum(axis=1) <= -1 + 1e-12).all()
+
+
+@pytest.mark.parametrize("order", [1, 2, 3, 4])
+def test_orthonormal_mass_matrix_matches_exact_integrals(order):
+    M = refelement.mass_matrix(order)
+    w = refelement.integration_weights(order)
+    assert np.allclose(M.sum(axis=1), w, atol=1e-13)
+    assert w.sum() == pytest.approx(4 / 3, rel=1e-14)
+
+
+def test_variance_like_the_reference():
+    """test_pyrticle.py:13-35 (Welford variance with a 1e9 offset)."""
+    for entire in (False, True):
+        data = [4, 7, 13, 16]
+        want = np.var(data, ddof=0 if entire else 1)
+        for d in (data, [1e9 + x for x in data]):
+            sg = StatsGatherer()
+            for x in d:
+                sg.add(x)
+            got = sg.variance() if entire else sg.variance_sample()
+            assert abs(got - want) < 1e-15 * max(1, want) * (1e9 if d[0] > 1e8 else 1)
+
+
+def test_stats_merge_equals_sequential():
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=1000)
+    a, b = StatsGatherer(), StatsGatherer()
+    for v in x:
+        a.add(v)
+    b.add_moments(len(x), x.sum(), (x * x).sum(), x.min(), x.max())
+    assert b.mean() == pytest.approx(a.mean(), rel=1e-12)
+    assert b.variance() == pytest.approx(a.variance(), rel=1e-10)
+
+
+def test_lsrk4_is_fourth_order():
+    """The 2N-storage scheme integrates y' = y to 4th order."""
+    def run(nsteps):
+        y, k, dt = 1.0, 0.0, 1.0 / nsteps
+        for _ in range(nsteps):
+            for a, b in zip(LSRK4_A, LSRK4_B):
+                k = a * k + dt * y
+                y = y + b * k
+        return abs(y - math.e)
+    e1, e2 = run(10), run(20)
+    assert 14 < e1 / e2 < 18
+
+
+def test_box_mesh_tables_consistent():
+    m = meshgen.box_mesh((4, 3, 5), jitter=0.15, seed=4)
+    assert m.jacobians.sum() * 4 / 3 == pytest.approx(0.01 * 0.01 * 0.04, rel=1e-12)
+    for e in range(0, m.element_count, 7):
+        for f in range(4):
+            nb = m.face_neighbors[e, f]
+            if nb == meshgen.INVALID_ELEMENT:
+                continue
+            g = list(m.face_neighbors[nb]).index(e)
+            assert np.allclose(m.face_normals[e, f], -m.face_normals[nb, g])
+    # inverse maps take vertices to the reference vertices
+    p = m.points[m.elements[0]]
+    A = m.inverse_maps[0, :9].reshape(3, 3)
+    ref = (A @ p.T).T + m.inverse_maps[0, 9:]
+    assert np.allclose(ref, [[-1, -1, -1], [1, -1, -1], [-1, 1, -1], [-1, -1, 1]], atol=1e-12)
+
+
+def test_grid_remap_reproduces_kept_polynomials():
+    """I_e (w f(grid)) = f(nodes) for f in the span of the kept modes (grid.py:217-273)."""
+    mesh = meshgen.box_mesh((3, 3, 6), jitter=0.1, seed=2)
+    order = 2
+    brk = BrickInfo(0, 0, np.array([0.01, 0.01, 0.04]) / [12, 12, 48], [0, 0, 0], [12, 12, 48])
+    starts, gidx, pts, w = find_points_in_elements(mesh, [brk], 0.12)
+    mats, mstarts, kept = basis_reduction_matrices(mesh, order, starts, pts, w)
+    nodes = meshgen.element_nodes(mesh, order).reshape(mesh.element_count, -1, 3)
+    Np = refelement.node_count(order)
+    for e in range(0, mesh.element_count, 5):
+        P = starts[e + 1] - starts[e]
+        I = mats[mstarts[e]:mstarts[e + 1]].reshape(Np, P, order="F")
+        # constants are always kept
+        f = np.ones(P)
+        assert np.allclose(I @ (w[starts[e]:starts[e + 1]] * f), np.ones(Np), atol=1e-10)
+        assert 1 <= kept[e] <= min(Np, P)
+
+
+def test_workload_generators_are_seeded():
+    a = problems.make("config0", scale=0.01)
+    b = problems.make("config0", scale=0.01)
+    assert np.array_equal(a.positions, b.positions) and np.array_equal(a.fields, b.fields)
+    r = np.hypot(a.positions[:, 0] - 0.005, a.positions[:, 1] - 0.005)
+    assert r.max() < 0.0025
