@@ -116,7 +116,8 @@ def build_method(w, torch):
 
 
 def count_pairs(m, state, sf):
-    """Exact number of (particle, node) pairs inside the radius (one call)."""
+    """Exact (particle, position) and (particle, node) pair counts inside the
+    radius (one extra deposition call)."""
     from pyrticle_b200 import _lib
     import torch
     nn = len(m.discretization)
@@ -127,7 +128,7 @@ def count_pairs(m, state, sf):
         _lib.ShapeFunctionDesc(sf.radius, sf.exponent, sf.normalizer), None, len(state),
         state.x.data_ptr(), state.q.data_ptr(), None, state.el.data_ptr(), rho.data_ptr(),
         None, 0, C.byref(st), C.c_void_p(torch.cuda.current_stream().cuda_stream)))
-    return int(st.pair_count)
+    return int(st.pair_count), int(st.node_pair_count), int(st.evaluated_pairs)
 
 
 def timing_read(m, cat, reset=True):
@@ -273,7 +274,7 @@ def main():
     for _ in range(args.warmup):
         one_step()
     torch.cuda.synchronize()
-    pairs = count_pairs(m, s, sf)
+    pairs, node_pairs, evaluated = count_pairs(m, s, sf)
 
     # ---- timed region (device events, max over ranks) ----
     clocks = ClockSampler(local)
@@ -365,8 +366,10 @@ def main():
                 "traffic": None,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 pipe; "
                                "MEASURED_PEAKS.json has no FP64 figure)",
-                "algorithmic": f"15 flops x {pairs} (particle,node) pairs within the radius "
-                               f"per launch; {avg_gather:.3f} ms per launch",
+                "algorithmic": f"15 flops x {pairs} (particle, distinct node position) "
+                               f"pairs within the radius per launch ({node_pairs} "
+                               f"(particle, node) pairs over all DG nodes; coincident "
+                               f"nodes are evaluated once); {avg_gather:.3f} ms per launch",
                 "secondary": {"bound": "hbm", "kernel": "lsrk_stage_kernel<3>",
                               "achieved": stage_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                               "frac": stage_gbs / peaks["hbm_gbs"],
@@ -386,11 +389,13 @@ def main():
                                       "all-reduce of rho/j" if world > 1 else "1 GPU"},
             "clocks": clk, "gpu_launches": None, "roofline": roofline,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kernel.items()},
-            "pairs_per_deposition": pairs}
+            "pairs_per_deposition": {"positions": pairs, "nodes": node_pairs,
+                                     "evaluated": evaluated}}
     # libprt's own kernels in the timed region (CUB's radix-sort kernels not
     # counted): per sort iota + 7 permutation gathers; per RK stage one fused
-    # kernel; per deposition bin keys, bin starts, payload and the gather.
-    line["gpu_launches"] = int(kernel["lsrk_stage"][1] + kernel["deposit_gather"][1] +
+    # kernel; per deposition bin keys, bin starts, payload, the gather and
+    # the expansion to nodes.
+    line["gpu_launches"] = int(kernel["lsrk_stage"][1] + 2 * kernel["deposit_gather"][1] +
                                3 * kernel["deposit_stage"][1] + 8 * kernel["sort"][1])
     if e2e:
         line["e2e"] = e2e

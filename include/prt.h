@@ -218,8 +218,13 @@ enum prt_deposit_mode {
 typedef struct prt_deposit_stats {
   double norm_count, norm_sum, norm_sum_sq, norm_min, norm_max;
   double el_count, el_sum, el_sum_sq, el_min, el_max;
-  /* number of (particle, node) pairs with |x_node - x_p| <= radius */
+  /* (particle, position) pairs within the radius, over distinct node
+   * positions (what the device evaluates: coincident DG nodes share one) */
   double pair_count;
+  /* (particle, node) pairs within the radius, over all DG nodes */
+  double node_pair_count;
+  /* (particle, position) pairs the kernel evaluated (after culling) */
+  double evaluated_pairs;
 } prt_deposit_stats;
 
 /* Replaces deposit_rho / deposit_j / deposit_densities(dep, ds, ps,
@@ -228,8 +233,12 @@ typedef struct prt_deposit_stats {
  * wrap_depositor.cpp:44-50):
  *   rho[n]    = sum_p w_p S(x_n - x_p),  j[c][n] = sum_p w_p v_p[c] S(x_n - x_p)
  * with w_p = q_p (plain) or q_p / (sum_e |J_e| sum_i w_i S(x_i - x_p))
- * (normalised, `integral_weights` [Np] = M 1). rho or j may be NULL. The sum
- * is deterministic: no floating-point atomics, fixed order.
+ * (normalised, `integral_weights` [Np] = M 1, a HOST array). rho or j may
+ * be NULL. The sum is deterministic: no floating-point atomics, fixed order.
+ * Coincident DG nodes (shared faces, edges, vertices) are evaluated once and
+ * receive the same values. For the normalising mode the statistics count, per
+ * particle, the node positions within the radius (the reference counts the
+ * elements its walk visits, dep_normshape.hpp:176-177).
  * Particles with element PRT_INVALID_ELEMENT are skipped. When `stats` is
  * not NULL the call also counts the (particle, node) pairs inside the
  * radius, and synchronises `stream`. */

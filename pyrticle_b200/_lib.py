@@ -86,7 +86,8 @@ class ShapeFunctionDesc(C.Structure):
 class DepositStats(C.Structure):
     _fields_ = [(n, C.c_double) for n in (
         "norm_count", "norm_sum", "norm_sum_sq", "norm_min", "norm_max",
-        "el_count", "el_sum", "el_sum_sq", "el_min", "el_max", "pair_count")]
+        "el_count", "el_sum", "el_sum_sq", "el_min", "el_max", "pair_count",
+        "node_pair_count", "evaluated_pairs")]
 
 
 class Brick(C.Structure):

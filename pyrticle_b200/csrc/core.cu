@@ -123,7 +123,7 @@ extern "C" int prt_mesh_create(const prt_mesh_desc *d, prt_mesh **out) {
     D.bin_inv[a] = d->bin_inv_width[a];
     D.bin_dims[a] = d->bin_dims[a];
   }
-  if (rc == PRT_OK) rc = prt_mesh_build_tiles(m, d);
+  if (rc == PRT_OK) rc = prt_mesh_build_positions(m, d);
   if (rc != PRT_OK) {
     prt_mesh_destroy(m);
     return rc;
@@ -134,13 +134,14 @@ extern "C" int prt_mesh_create(const prt_mesh_desc *d, prt_mesh **out) {
 
 extern "C" int prt_mesh_destroy(prt_mesh *m) {
   if (!m) return PRT_OK;
+  const PositionSet &P = m->positions;
   const void *ptrs[] = {m->dev.inv_maps, m->dev.jacobians, m->dev.normals,
                         m->dev.plane_rhs, m->dev.neighbors, m->dev.axes,
                         m->dev.el_verts, m->dev.verts, m->dev.vadj_starts,
                         m->dev.vadj, m->dev.nodes, m->dev.bin_starts,
                         m->dev.bin_elements, m->face_centroids, m->face_radii,
-                        m->tile_boxes, m->el_spheres, m->tile_bins.starts,
-                        m->tile_bins.tiles};
+                        P.pos, P.node_to_pos, P.run_starts, P.run_nodes, P.tile_boxes,
+                        P.group_starts, P.group_spheres, P.bins.starts, P.bins.tiles};
   for (const void *p : ptrs)
     if (p) cudaFree((void *)p);
   delete m;
@@ -464,8 +465,11 @@ __global__ void __launch_bounds__(256)
 
 // One fused stage: velocity, interpolation, Lorentz force, 2N-storage RK
 // update, relocation. Dead particles (PRT_INVALID) are not touched.
+// resident 256-thread CTAs per SM the stage kernel is compiled for: the
+// kernel is latency-bound, so occupancy matters more than registers, up to
+// order 3; order 4 (35 monomials in registers) keeps the larger budget
 template <int ORDER>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, ORDER >= 4 ? 2 : 3)
     lsrk_stage_kernel(DevMesh M, const Lagrange<ORDER> L, Fields6 F, long long n,
                       double *__restrict__ x, double *__restrict__ p,
                       const double *__restrict__ q, const double *__restrict__ mass,
@@ -671,7 +675,7 @@ __global__ void iota_kernel(long long n, uint32_t *__restrict__ v) {
 }
 
 template <class T, int C>
-__global__ void gather_kernel(long long n, const uint32_t *__restrict__ perm,
+__global__ void permute_kernel(long long n, const uint32_t *__restrict__ perm,
                               const T *__restrict__ src, T *__restrict__ dst) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -687,7 +691,7 @@ static int permute(prt_workspace *ws, long long n, const uint32_t *perm, T *arr,
   int rc;
   T *tmp = (T *)ws_buffer(ws, PRT_WS_SORT_TMP, sizeof(T) * C * (size_t)n, &rc);
   if (!tmp) return rc;
-  gather_kernel<T, C><<<prt_grid_blocks(n, 256), 256, 0, s>>>(n, perm, arr, tmp);
+  permute_kernel<T, C><<<prt_grid_blocks(n, 256), 256, 0, s>>>(n, perm, arr, tmp);
   PRT_CHECK_CUDA(cudaGetLastError());
   PRT_CHECK_CUDA(
       cudaMemcpyAsync(arr, tmp, sizeof(T) * C * (size_t)n, cudaMemcpyDeviceToDevice, s));

@@ -1,77 +1,43 @@
-// deposit.cu -- shape-function deposition onto DG nodes and onto brick grids,
-// and the grid -> mesh remap.
+// deposit.cu -- shape-function deposition onto DG nodes.
 //
 // The reference deposits particle by particle: a face-connected walk from
 // the particle's element visits every element its shape ball reaches and
 // scatters q S(x_node - x_p) into rho/j (dep_shape.hpp:128-149,
 // element_finder.hpp:239-293). The walk reaches exactly the elements that
 // intersect the ball (on a convex mesh), and S vanishes at and beyond the
-// radius, so the result is the sum, over every node, of the contributions of
-// every particle within one radius of it. This file computes that sum as a
-// gather, which needs no floating-point atomics and is deterministic:
+// radius, so the result is, for every node, the sum of the contributions of
+// every particle within one radius of it. That value depends only on the
+// node's position, and DG nodes on shared faces, edges and vertices are
+// coincident (order 3: about 4.3 distinct positions per tetrahedron for 20
+// nodes). This file computes the sum as a gather over the distinct
+// positions, which needs no floating-point atomics and is deterministic:
 //
-//   1. bin the particles on a uniform grid (bin width >= radius), radix sort
-//      by bin (stable), gather a 64-byte payload per particle in bin order;
-//   2. one CTA per tile of consecutive elements (<= 128 nodes, one node per
-//      thread): stream the particles of the bins that overlap the tile box
-//      grown by the radius through shared memory, cull each against the
-//      bounding sphere of each element of the tile, and accumulate
-//      rho, j_x, j_y, j_z in registers in fixed (bin, particle) order;
-//   3. write the node sums once (coalesced).
+//   1. set-up (host, once per mesh): merge coincident nodes into positions,
+//      order them along a Morton curve; 32 consecutive positions form a warp
+//      group (bounding sphere), 128 a CTA tile (bounding box);
+//   2. per call: bin the particles (bin width radius/2), radix sort by bin,
+//      pack a 64-byte payload per particle in bin order;
+//   3. one CTA per tile: stream the particles of the bin rows within the
+//      radius of the tile box through shared memory; each warp compacts the
+//      particles inside its sphere grown by the radius into its own buffer
+//      and all 32 lanes walk that buffer (one position per lane), with a
+//      branchless weight; rho, j accumulate in registers in bin order;
+//   4. expand: every node takes its position's values.
 //
-// Periodic axes are handled with particle images shifted by the period, the
-// same images the walk uses when it crosses a periodic face.
+// Periodic axes use particle images shifted by the period, the images the
+// walk uses when it crosses a periodic face.
 
 #include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <numeric>
 #include <vector>
 
-#include "common.cuh"
-#include "handles.cuh"
+#include "binning.cuh"
 
-namespace {
-
-constexpr int CHUNK = 128;      // particles staged per shared-memory round
-constexpr int PAYLOAD = 8;      // doubles per staged particle
-constexpr int BLOCK = 128;      // threads per deposition CTA
-
-struct BinGrid {
-  double origin[3];
-  double inv_w[3];
-  int dims[3];
-  int periodic[3];
-  double period[3];
-  long long nbins;
-};
-
-// Particle payload: x, y, z, w, w vx, w vy, w vz, tag (tag: brick id or 0).
-struct DepParticles {
-  const double *__restrict__ payload;  // [count][8], bin order
-  const uint32_t *__restrict__ starts; // [nbins + 1]
-};
-
-__device__ __forceinline__ int bin_coord(const BinGrid &G, int d, double x) {
-  double u = (x - G.origin[d]) * G.inv_w[d];
-  if (!(u >= 0.0)) return 0;
-  if (u >= (double)G.dims[d]) return G.dims[d] - 1;
-  return min((int)u, G.dims[d] - 1);
-}
-
-// unwrapped bin index of a coordinate, unclamped (for candidate ranges)
-__device__ __forceinline__ int bin_floor(const BinGrid &G, int d, double x) {
-  double u = floor((x - G.origin[d]) * G.inv_w[d]);
-  u = fmax(fmin(u, 1e9), -1e9);
-  return (int)u;
-}
-
-__device__ __forceinline__ int floor_div(int a, int b) {
-  int q = a / b;
-  if ((a % b != 0) && ((a < 0) != (b < 0))) --q;
-  return q;
-}
+namespace prt_dep {
 
 __global__ void bin_keys_kernel(BinGrid G, long long n, const double *__restrict__ x,
                                 const uint32_t *__restrict__ el,
@@ -94,8 +60,7 @@ __global__ void bin_starts_kernel(long long nbins, long long n,
                                   uint32_t *__restrict__ starts) {
   long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (b > nbins) return;
-  // lower_bound of b in sorted_keys
-  long long lo = 0, hi = n;
+  long long lo = 0, hi = n;  // lower_bound of b
   while (lo < hi) {
     long long mid = (lo + hi) >> 1;
     if ((long long)sorted_keys[mid] < b)
@@ -106,452 +71,50 @@ __global__ void bin_starts_kernel(long long nbins, long long n,
   starts[b] = (uint32_t)lo;
 }
 
-// payload in bin order; weight[i] multiplies q (plain: normaliser; normalised:
-// normaliser / integral, zero for a zero integral).
-__global__ void payload_kernel(long long count, const uint32_t *__restrict__ perm,
-                               long long n, const double *__restrict__ x,
-                               const double *__restrict__ q,
+__global__ void payload_kernel(long long n, const uint32_t *__restrict__ perm,
+                               const double *__restrict__ x, const double *__restrict__ q,
                                const double *__restrict__ v,
                                const double *__restrict__ scale, double normalizer,
-                               const uint32_t *__restrict__ tag,
-                               double *__restrict__ out) {
+                               const uint32_t *__restrict__ tag, double *__restrict__ out) {
   long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (s >= count) return;
+  if (s >= n) return;
   uint32_t i = perm[s];
   double w = scale ? scale[i] * normalizer : q[i] * normalizer;
-  double *o = out + PAYLOAD * s;
-  o[0] = x[i];
-  o[1] = x[n + i];
-  o[2] = x[2 * n + i];
-  o[3] = w;
+  double2 *o = reinterpret_cast<double2 *>(out + PAYLOAD * s);
+  double v0 = 0, v1 = 0, v2 = 0;
   if (v) {
-    o[4] = w * v[i];
-    o[5] = w * v[n + i];
-    o[6] = w * v[2 * n + i];
-  } else {
-    o[4] = o[5] = o[6] = 0;
+    v0 = w * v[i];
+    v1 = w * v[n + i];
+    v2 = w * v[2 * n + i];
   }
-  o[7] = tag ? (double)tag[i] : 0.0;
+  o[0] = make_double2(x[i], x[n + i]);
+  o[1] = make_double2(x[2 * n + i], w);
+  o[2] = make_double2(v0, v1);
+  o[3] = make_double2(v2, tag ? (double)tag[i] : 0.0);
 }
 
-// ---------------------------------------------------------------- targets
-
-// Tile of consecutive mesh elements; groups = elements (bounding-sphere cull).
-struct MeshTarget {
-  const double *__restrict__ nodes;    // [Nn][3]
-  const double *__restrict__ boxes;    // [tiles][6]
-  const double *__restrict__ spheres;  // [E][4]
-  long long E;
-  int Np;
-  int tile_elements;
-  long long node_count;
-
-  __device__ int groups(long long tile) const {
-    long long e0 = tile * tile_elements;
-    return (int)min((long long)tile_elements, E - e0);
-  }
-  __device__ int items(long long tile) const { return groups(tile) * Np; }
-  __device__ long long out_index(long long tile, int t) const {
-    return tile * tile_elements * Np + t;
-  }
-  __device__ void point(long long tile, int t, double &x0, double &x1, double &x2) const {
-    const double *p = nodes + 3 * out_index(tile, t);
-    x0 = p[0];
-    x1 = p[1];
-    x2 = p[2];
-  }
-  __device__ int group_of(int t) const { return t / Np; }
-  __device__ void box(long long tile, double lo[3], double hi[3]) const {
-    const double *b = boxes + 6 * tile;
-    lo[0] = b[0]; lo[1] = b[1]; lo[2] = b[2];
-    hi[0] = b[3]; hi[1] = b[4]; hi[2] = b[5];
-  }
-  // sphere of group g: centre and squared cull radius (radius + R_e)^2
-  __device__ void group_sphere(long long tile, int g, double radius, double s[4]) const {
-    const double *sp = spheres + 4 * (tile * tile_elements + g);
-    s[0] = sp[0];
-    s[1] = sp[1];
-    s[2] = sp[2];
-    double r = radius + sp[3];
-    s[3] = r * r;
-  }
-  __device__ bool tag_ok(long long, double) const { return true; }
-};
-
-// Tile of 8 x 4 x 4 points of one brick; one group (the tile box).
-struct BrickTarget {
-  const prt_brick *__restrict__ bricks;
-  const long long *__restrict__ tile_starts;  // [bricks+1] cumulative tile counts
-  int brick_count;
-  int check_tag;
-
-  __device__ int find_brick(long long tile) const {
-    int b = 0;
-    while (b + 1 < brick_count && tile_starts[b + 1] <= tile) ++b;
-    return b;
-  }
-  __device__ void tile_origin(long long tile, int &b, int i0[3]) const {
-    b = find_brick(tile);
-    const prt_brick &B = bricks[b];
-    long long local = tile - tile_starts[b];
-    int tx = (B.dims[0] + 7) / 8, ty = (B.dims[1] + 3) / 4;
-    i0[0] = (int)(local % tx) * 8;
-    i0[1] = (int)((local / tx) % ty) * 4;
-    i0[2] = (int)(local / ((long long)tx * ty)) * 4;
-  }
-  __device__ int groups(long long) const { return 1; }
-  __device__ int items(long long) const { return 128; }
-  __device__ bool valid(long long tile, int t, int &b, int idx[3]) const {
-    int i0[3];
-    tile_origin(tile, b, i0);
-    idx[0] = i0[0] + (t & 7);
-    idx[1] = i0[1] + ((t >> 3) & 3);
-    idx[2] = i0[2] + (t >> 5);
-    const prt_brick &B = bricks[b];
-    return idx[0] < B.dims[0] && idx[1] < B.dims[1] && idx[2] < B.dims[2];
-  }
-  __device__ long long out_index(long long tile, int t) const {
-    int b, idx[3];
-    if (!valid(tile, t, b, idx)) return -1;
-    const prt_brick &B = bricks[b];
-    return B.start_index + idx[0] + (long long)B.dims[0] * (idx[1] + (long long)B.dims[1] * idx[2]);
-  }
-  __device__ void point(long long tile, int t, double &x0, double &x1, double &x2) const {
-    int b, idx[3];
-    valid(tile, t, b, idx);
-    const prt_brick &B = bricks[b];
-    x0 = B.origin[0] + B.stepwidths[0] / 2 + idx[0] * B.stepwidths[0];
-    x1 = B.origin[1] + B.stepwidths[1] / 2 + idx[1] * B.stepwidths[1];
-    x2 = B.origin[2] + B.stepwidths[2] / 2 + idx[2] * B.stepwidths[2];
-  }
-  __device__ int group_of(int) const { return 0; }
-  __device__ void box(long long tile, double lo[3], double hi[3]) const {
-    int b, i0[3];
-    tile_origin(tile, b, i0);
-    const prt_brick &B = bricks[b];
-    for (int d = 0; d < 3; ++d) {
-      int cnt = d == 0 ? 8 : 4;
-      int last = min(i0[d] + cnt, B.dims[d]) - 1;
-      lo[d] = B.origin[d] + B.stepwidths[d] / 2 + i0[d] * B.stepwidths[d];
-      hi[d] = B.origin[d] + B.stepwidths[d] / 2 + last * B.stepwidths[d];
-    }
-  }
-  __device__ void group_sphere(long long tile, int, double radius, double s[4]) const {
-    double lo[3], hi[3];
-    box(tile, lo, hi);
-    double hx = 0.5 * (hi[0] - lo[0]), hy = 0.5 * (hi[1] - lo[1]), hz = 0.5 * (hi[2] - lo[2]);
-    s[0] = lo[0] + hx;
-    s[1] = lo[1] + hy;
-    s[2] = lo[2] + hz;
-    double r = radius + sqrt(hx * hx + hy * hy + hz * hz);
-    s[3] = r * r;
-  }
-  __device__ bool tag_ok(long long tile, double tag) const {
-    if (!check_tag) return true;
-    return (long long)tag == (long long)find_brick(tile);
-  }
-};
-
-enum Weight { W_SHAPE2 = 0, W_SHAPE_POW = 1, W_TRILINEAR = 2 };
-
-struct ShapeParams {
-  double radius, radius2, inv_radius, alpha;
-  double reach[3];  // candidate reach per axis (radius, or h for trilinear)
-};
-
-// The gather kernel. One CTA per tile, one target point per thread.
-template <class Target, int WEIGHT, bool COUNT = false>
-__global__ void __launch_bounds__(BLOCK)
-    gather_kernel(Target T, BinGrid G, DepParticles P, ShapeParams S,
-                  double *__restrict__ rho, double *__restrict__ j, long long j_stride,
-                  const prt_brick *__restrict__ tri_bricks,
-                  unsigned long long *__restrict__ pair_counter) {
-  __shared__ double sp[PAYLOAD][CHUNK + 1];
-  __shared__ uint32_t smask[CHUNK];
-  __shared__ double sph[32][4];
-
-  const long long tile = blockIdx.x;
-  const int t = threadIdx.x;
-  const int ng = T.groups(tile);
-  const int ni = T.items(tile);
-  const bool mine = t < ni;
-  long long oidx = mine ? T.out_index(tile, t) : -1;
-  const bool live = mine && oidx >= 0;
-  double x0 = 0, x1 = 0, x2 = 0;
-  if (live) T.point(tile, t, x0, x1, x2);
-  const int grp = live ? T.group_of(t) : 0;
-  if (t < ng) T.group_sphere(tile, t, S.radius, sph[t]);
-
-  // trilinear: the point's brick and index for the clamped hat weights
-  int tb = 0, tidx[3] = {0, 0, 0};
-  double th[3] = {1, 1, 1};
-  if constexpr (WEIGHT == W_TRILINEAR) {
-    if (live) {
-      T.valid(tile, t, tb, tidx);
-      for (int d = 0; d < 3; ++d) th[d] = tri_bricks[tb].stepwidths[d];
-    }
-  }
-
-  double a_rho = 0, a_jx = 0, a_jy = 0, a_jz = 0;
-  unsigned long long npairs = 0;
-
-  double lo[3], hi[3];
-  T.box(tile, lo, hi);
-  int u0[3], u1[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    u0[d] = bin_floor(G, d, lo[d] - S.reach[d]);
-    u1[d] = bin_floor(G, d, hi[d] + S.reach[d]);
-    if (G.periodic[d]) {
-      u0[d] -= 1;
-      u1[d] += 1;
-    } else {
-      u0[d] = max(u0[d], 0);
-      u1[d] = min(u1[d], G.dims[d] - 1);
-    }
-  }
-  __syncthreads();
-
-  for (int bz = u0[2]; bz <= u1[2]; ++bz) {
-    int wz = bz, qz = 0;
-    if (G.periodic[2]) { qz = floor_div(bz, G.dims[2]); wz = bz - qz * G.dims[2]; }
-    const double sz = qz * G.period[2];
-    for (int by = u0[1]; by <= u1[1]; ++by) {
-      int wy = by, qy = 0;
-      if (G.periodic[1]) { qy = floor_div(by, G.dims[1]); wy = by - qy * G.dims[1]; }
-      const double sy = qy * G.period[1];
-      // the x-row splits into segments of constant shift
-      int bx = u0[0];
-      while (bx <= u1[0]) {
-        int wx = bx, qx = 0, seg_end = u1[0];
-        if (G.periodic[0]) {
-          qx = floor_div(bx, G.dims[0]);
-          wx = bx - qx * G.dims[0];
-          seg_end = min(u1[0], (qx + 1) * G.dims[0] - 1);
-        }
-        const double sx = qx * G.period[0];
-        const long long row = (long long)G.dims[0] * (wy + (long long)G.dims[1] * wz);
-        const uint32_t s0 = P.starts[row + wx];
-        const uint32_t s1 = P.starts[row + wx + (seg_end - bx) + 1];
-        bx = seg_end + 1;
-        for (uint32_t c0 = s0; c0 < s1; c0 += CHUNK) {
-          const int cnt = (int)min((uint32_t)CHUNK, s1 - c0);
-          __syncthreads();
-          for (int k = t; k < cnt * PAYLOAD; k += BLOCK) {
-            double val = P.payload[(size_t)c0 * PAYLOAD + k];
-            const int comp = k % PAYLOAD;
-            if (comp == 0) val += sx;
-            if (comp == 1) val += sy;
-            if (comp == 2) val += sz;
-            sp[comp][k / PAYLOAD] = val;
-          }
-          __syncthreads();
-          for (int k = t; k < cnt; k += BLOCK) {
-            const double px = sp[0][k], py = sp[1][k], pz = sp[2][k];
-            uint32_t m = 0;
-            if (T.tag_ok(tile, sp[7][k])) {
-              for (int g = 0; g < ng; ++g) {
-                double dx = px - sph[g][0], dy = py - sph[g][1], dz = pz - sph[g][2];
-                if (dx * dx + dy * dy + dz * dz <= sph[g][3]) m |= 1u << g;
-              }
-            }
-            smask[k] = m;
-          }
-          __syncthreads();
-          if (live) {
-            const uint32_t bit = 1u << grp;
-            for (int k = 0; k < cnt; ++k) {
-              if (!(smask[k] & bit)) continue;
-              const double dx = x0 - sp[0][k];
-              const double dy = x1 - sp[1][k];
-              const double dz = x2 - sp[2][k];
-              double s;
-              if constexpr (WEIGHT == W_TRILINEAR) {
-                // clamped hat weight per axis (edge points absorb the outside)
-                double wgt = 1.0;
-                const double dd[3] = {dx, dy, dz};
-                const prt_brick &B = tri_bricks[tb];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                  const double u = -dd[d] / th[d];  // (x_p - pt) / h
-                  // edge points also take the weight of the missing neighbour
-                  const bool edge = (tidx[d] == 0 && u < 0) || (tidx[d] == B.dims[d] - 1 && u > 0);
-                  wgt *= edge ? 1.0 : fmax(0.0, 1.0 - fabs(u));
-                }
-                if (wgt == 0) continue;
-                s = wgt;
-              } else {
-                const double r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 > S.radius2) continue;
-                if (COUNT) ++npairs;
-                const double rt = S.radius - r2 * S.inv_radius;
-                s = WEIGHT == W_SHAPE2 ? rt * rt : pow(rt, S.alpha);
-              }
-              a_rho = fma(sp[3][k], s, a_rho);
-              a_jx = fma(sp[4][k], s, a_jx);
-              a_jy = fma(sp[5][k], s, a_jy);
-              a_jz = fma(sp[6][k], s, a_jz);
-            }
-          }
-        }
-      }
-    }
-  }
-  if (COUNT) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) npairs += __shfl_down_sync(0xffffffffu, npairs, o);
-    if ((t & 31) == 0 && npairs) atomicAdd(pair_counter, npairs);
-  }
-  if (live) {
-    if (rho) rho[oidx] = a_rho;
-    if (j) {
-      j[oidx] = a_jx;
-      j[j_stride + oidx] = a_jy;
-      j[2 * j_stride + oidx] = a_jz;
-    }
-  }
-}
-
-// Normalising pre-pass (dep_normshape.hpp:125-199): per particle, the
-// integral sum_e |J_e| sum_i w_i S(x_i - x_p) over every element with a node
-// inside the ball, gathered one warp per particle over the element bins of
-// the tiles; scale = q / integral (0 and a warning for a zero integral).
-struct TileBins {
-  double origin[3], inv_w[3];
-  int dims[3];
-  const uint32_t *__restrict__ starts;
-  const uint32_t *__restrict__ tiles;
-};
-
-template <bool ALPHA2>
-__global__ void normalize_kernel(DevMesh M, TileBins TB, const double *__restrict__ boxes,
-                                 const double *__restrict__ spheres, int tile_elements,
-                                 const double *__restrict__ iw, ShapeParams S,
-                                 double normalizer, long long n,
-                                 const double *__restrict__ x, const double *__restrict__ q,
-                                 const uint32_t *__restrict__ el,
-                                 double *__restrict__ scale_out,
-                                 double *__restrict__ elcount_out, DevStatus *st) {
-  const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const long long i = warp;
-  if (el && el[i] == PRT_INVALID) {
-    if (lane == 0) {
-      scale_out[i] = 0;
-      elcount_out[i] = -1;
-    }
-    return;
-  }
-  const double px = x[i], py = x[n + i], pz = x[2 * n + i];
-  const int Np = M.Np;
-  double integral = 0;
-  int elements_hit = 0;
-  // images on periodic axes
-  int lo_img[3], hi_img[3];
-  for (int d = 0; d < 3; ++d) {
-    lo_img[d] = hi_img[d] = 0;
-    if (M.pmin[d] != M.pmax[d]) {
-      const double pd = d == 0 ? px : (d == 1 ? py : pz);
-      if (pd - S.radius < M.pmin[d]) hi_img[d] = 1;
-      if (pd + S.radius > M.pmax[d]) lo_img[d] = -1;
-    }
-  }
-  for (int iz = lo_img[2]; iz <= hi_img[2]; ++iz)
-    for (int iy = lo_img[1]; iy <= hi_img[1]; ++iy)
-      for (int ix = lo_img[0]; ix <= hi_img[0]; ++ix) {
-        const double cx = px + ix * (M.pmax[0] - M.pmin[0]);
-        const double cy = py + iy * (M.pmax[1] - M.pmin[1]);
-        const double cz = pz + iz * (M.pmax[2] - M.pmin[2]);
-        const double c[3] = {cx, cy, cz};
-        int b0[3], b1[3];
-        for (int d = 0; d < 3; ++d) {
-          double l = floor((c[d] - S.radius - TB.origin[d]) * TB.inv_w[d]);
-          double h = floor((c[d] + S.radius - TB.origin[d]) * TB.inv_w[d]);
-          b0[d] = (int)fmax(0.0, fmin(l, TB.dims[d] - 1.0));
-          b1[d] = (int)fmax(0.0, fmin(h, TB.dims[d] - 1.0));
-        }
-        for (int bz = b0[2]; bz <= b1[2]; ++bz)
-          for (int by = b0[1]; by <= b1[1]; ++by)
-            for (int bx = b0[0]; bx <= b1[0]; ++bx) {
-              const long long bid = bx + (long long)TB.dims[0] * (by + (long long)TB.dims[1] * bz);
-              for (uint32_t k = TB.starts[bid]; k < TB.starts[bid + 1]; ++k) {
-                const uint32_t tile = TB.tiles[k];
-                const double *bx6 = boxes + 6 * (size_t)tile;
-                // dedupe: a tile is handled in the first bin of the overlap
-                // of its bin range and the particle's bin range
-                int first[3];
-                for (int d = 0; d < 3; ++d) {
-                  double l = floor((bx6[d] - TB.origin[d]) * TB.inv_w[d]);
-                  int tl = (int)fmax(0.0, fmin(l, TB.dims[d] - 1.0));
-                  first[d] = max(tl, b0[d]);
-                }
-                if (bx != first[0] || by != first[1] || bz != first[2]) continue;
-                // box-ball test
-                double d2 = 0;
-                for (int d = 0; d < 3; ++d) {
-                  double e = fmax(0.0, fmax(bx6[d] - c[d], c[d] - bx6[3 + d]));
-                  d2 += e * e;
-                }
-                if (d2 > S.radius2) continue;
-                const long long e0 = (long long)tile * tile_elements;
-                const long long e1 = min(e0 + tile_elements, M.E);
-                for (long long e = e0; e < e1; ++e) {
-                  const double *sph = spheres + 4 * e;
-                  double dx = cx - sph[0], dy = cy - sph[1], dz = cz - sph[2];
-                  double rr = S.radius + sph[3];
-                  if (dx * dx + dy * dy + dz * dz > rr * rr) continue;
-                  double el_int = 0;
-                  bool any = false;
-                  for (int nd = lane; nd < Np; nd += 32) {
-                    const double *xn = M.nodes + 3 * (e * Np + nd);
-                    double ex = xn[0] - cx, ey = xn[1] - cy, ez = xn[2] - cz;
-                    double r2 = ex * ex + ey * ey + ez * ez;
-                    if (r2 <= S.radius2) {
-                      double rt = S.radius - r2 * S.inv_radius;
-                      double s = normalizer * (ALPHA2 ? rt * rt : pow(rt, S.alpha));
-                      el_int = fma(s, iw[nd], el_int);
-                      any = any || s != 0;
-                    }
-                  }
-                  integral = fma(el_int, M.jacobians[e], integral);
-                  if (__any_sync(0xffffffffu, any)) ++elements_hit;
-                }
-              }
-            }
-      }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) integral += __shfl_xor_sync(0xffffffffu, integral, o);
-  if (lane == 0) {
-    if (integral == 0) {
-      scale_out[i] = 0;
-      record_warning(st, PRT_WARN_ZERO_MASS, i);
-    } else {
-      scale_out[i] = q[i] / integral;
-    }
-    elcount_out[i] = elements_hit;
-  }
-}
-
-int choose_bins(const prt_mesh *m, double reach_x, BinGrid &G, int *rc) {
+int choose_bins(const prt_mesh *m, const double box_lo[3], const double box_hi[3],
+                double bin_width, double radius, BinGrid &G, int *rc) {
   *rc = PRT_OK;
   long long nb = 1;
   for (int d = 0; d < 3; ++d) {
     const bool per = m->dev.pmin[d] != m->dev.pmax[d];
     G.periodic[d] = per;
-    double lo = per ? m->dev.pmin[d] : m->box_lo[d];
-    double hi = per ? m->dev.pmax[d] : m->box_hi[d];
-    double ext = hi - lo;
-    double w = reach_x > 0 ? reach_x : ext;
+    const double lo = per ? m->dev.pmin[d] : box_lo[d];
+    const double hi = per ? m->dev.pmax[d] : box_hi[d];
+    const double ext = hi - lo;
+    const double w = bin_width > 0 ? bin_width : ext;
     int dims = ext > 0 ? (int)std::max(1.0, std::floor(ext / w)) : 1;
     dims = std::min(dims, 1024);
-    double width = ext > 0 ? ext / dims : 1.0;
-    if (per && reach_x * 2 >= ext) {
-      *rc = PRT_ERR_INVALID_ARGUMENT;  // ball reaches its own image
+    const double width = ext > 0 ? ext / dims : 1.0;
+    if (per && radius * 2 >= ext) {
+      *rc = PRT_ERR_INVALID_ARGUMENT;  // a ball would meet its own image
       return 0;
     }
     G.origin[d] = lo;
     G.inv_w[d] = 1.0 / width;
+    G.w[d] = width;
+    G.slack[d] = 1e-6 * width + 1e-9 * std::max(std::fabs(lo), std::fabs(hi));
     G.dims[d] = dims;
     G.period[d] = per ? ext : 0.0;
     nb *= dims;
@@ -564,12 +127,10 @@ int choose_bins(const prt_mesh *m, double reach_x, BinGrid &G, int *rc) {
   return 1;
 }
 
-// Bins, sorts and packs the live particles; fills P. `scale` (or NULL) and
-// `tag` (or NULL) feed the payload.
 int stage_particles(prt_workspace *ws, const BinGrid &G, long long n, const double *x,
                     const double *q, const double *v, const uint32_t *el,
                     const double *scale, double normalizer, const uint32_t *tag,
-                    DepParticles &P, long long *live_count, cudaStream_t s) {
+                    DepParticles &P, cudaStream_t s) {
   int rc;
   uint32_t *keys = (uint32_t *)ws_buffer(ws, PRT_WS_DEP_KEYS, 8 * (size_t)n, &rc);
   if (!keys) return rc;
@@ -596,31 +157,414 @@ int stage_particles(prt_workspace *ws, const BinGrid &G, long long n, const doub
   double *payload =
       (double *)ws_buffer(ws, PRT_WS_DEP_PARTICLES, sizeof(double) * PAYLOAD * (size_t)n, &rc);
   if (!payload) return rc;
-  // all n rows are packed; rows past starts[nbins] (dead particles) are never read
-  payload_kernel<<<prt_grid_blocks(n, 256), 256, 0, s>>>(n, vals_out, n, x, q, v, scale,
+  // rows past starts[nbins] (removed particles) are packed but never read
+  payload_kernel<<<prt_grid_blocks(n, 256), 256, 0, s>>>(n, vals_out, x, q, v, scale,
                                                          normalizer, tag, payload);
   PRT_CHECK_CUDA(cudaGetLastError());
   P.payload = payload;
   P.starts = starts;
-  if (live_count) *live_count = n;
   return PRT_OK;
 }
 
+}  // namespace prt_dep
+
+namespace {
+
+using namespace prt_dep;
+
+constexpr int WARPS = BLOCK / 32;
+
+// resident CTAs per SM the group kernel is compiled for (register budget)
+#ifndef PRT_GATHER_MIN_BLOCKS
+#define PRT_GATHER_MIN_BLOCKS 6
+#endif
+// per-warp ring of compacted particles (two batches of 32)
+constexpr int RING = 64;
+
+// One warp per position group (<= 32 positions, one per lane), warps fully
+// independent (no block-level barrier). The warp streams the particles of
+// the bin rows within its sphere grown by the radius straight from L2/L1:
+// each lane tests one particle on the payload's first 32-byte sector
+// (x, y, z, q N); the survivors' weights are fetched and appended to the
+// warp's shared-memory ring (warp ballot); every 32 entries the lanes walk
+// the batch, two particles per iteration. Coordinates are relative to the
+// group centre c: r^2 = |u|^2 + |w|^2 - 2 u.w with u = x_position - c,
+// w = x_particle - c. Output out[4][npos]: rho, j_x, j_y, j_z per position.
+// In COUNT mode counters[0] receives the (particle, position) pairs within
+// the radius, counters[1] the (particle, node) pairs (positions weighted by
+// their node count) and counters[2] the evaluated pairs.
+template <bool ALPHA2, bool COUNT>
+__global__ void __launch_bounds__(BLOCK, PRT_GATHER_MIN_BLOCKS)
+    deposit_groups_kernel(const double *__restrict__ pos, long long ngroups,
+                          const uint32_t *__restrict__ gstarts,
+                          const double *__restrict__ gspheres,
+                          const uint32_t *__restrict__ run_starts, BinGrid G,
+                          DepParticles P, ShapeParams S, long long npos,
+                          double *__restrict__ out, unsigned long long *__restrict__ counters) {
+  // ring entries: (wx, wy), (wz, |w|^2), (q N, q N vx), (q N vy, q N vz)
+  __shared__ double2 ring[WARPS][4][RING];
+
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long g = blockIdx.x * (long long)WARPS + wid;
+  if (g >= ngroups) return;  // whole warp
+  const uint32_t p0 = gstarts[g];
+  const int npg = (int)(gstarts[g + 1] - p0);
+  const bool live = lane < npg;
+  double2(*R)[RING] = ring[wid];
+
+  const double c0 = gspheres[4 * g], c1 = gspheres[4 * g + 1], c2 = gspheres[4 * g + 2];
+  const double reach = S.radius + gspheres[4 * g + 3];
+  const double cull2 = (reach * (1 + 1e-9)) * (reach * (1 + 1e-9));
+  double U0 = 0, U1 = 0, U2 = 0, A = 0;
+  unsigned mult = 0;
+  if (live) {
+    const long long u = p0 + lane;
+    const double u0 = pos[3 * u] - c0, u1 = pos[3 * u + 1] - c1, u2 = pos[3 * u + 2] - c2;
+    A = u0 * u0 + u1 * u1 + u2 * u2;
+    U0 = -2 * u0;
+    U1 = -2 * u1;
+    U2 = -2 * u2;
+    if (COUNT) mult = run_starts[u + 1] - run_starts[u];
+  }
+
+  double r0 = 0, x0 = 0, y0 = 0, z0 = 0, r1 = 0, x1 = 0, y1 = 0, z1 = 0;
+  unsigned long long npairs = 0, nnode = 0, nevals = 0;
+  const double neg_inv_a = -S.inv_radius, rad = S.radius, rad2 = S.radius2;
+
+  auto weight = [&](double r2) -> double {
+    const double tr = fma(r2, neg_inv_a, rad);
+    if (ALPHA2) {
+      const double tp = fmax(tr, 0.0);
+      return tp * tp;
+    }
+    return tr > 0 ? pow(tr, S.alpha) : 0.0;
+  };
+  int head = 0, count = 0;
+  // walks `k` ring entries from head (warp-uniform k)
+  auto drain = [&](int k) {
+    int i = 0;
+    for (; i + 1 < k; i += 2) {
+      const int ea = (head + i) & (RING - 1), eb = (head + i + 1) & (RING - 1);
+      const double2 pa = R[0][ea], qa = R[1][ea], pb = R[0][eb], qb = R[1][eb];
+      const double r2a = fma(U0, pa.x, fma(U1, pa.y, fma(U2, qa.x, A + qa.y)));
+      const double r2b = fma(U0, pb.x, fma(U1, pb.y, fma(U2, qb.x, A + qb.y)));
+      const double sa = weight(r2a), sb = weight(r2b);
+      const double2 wa = R[2][ea], va = R[3][ea], wb = R[2][eb], vb = R[3][eb];
+      r0 = fma(wa.x, sa, r0);
+      x0 = fma(wa.y, sa, x0);
+      y0 = fma(va.x, sa, y0);
+      z0 = fma(va.y, sa, z0);
+      r1 = fma(wb.x, sb, r1);
+      x1 = fma(wb.y, sb, x1);
+      y1 = fma(vb.x, sb, y1);
+      z1 = fma(vb.y, sb, z1);
+      if (COUNT) {
+        const unsigned ia = live && r2a <= rad2, ib = live && r2b <= rad2;
+        npairs += ia + ib;
+        nnode += (ia + ib) * mult;
+      }
+    }
+    if (i < k) {
+      const int ea = (head + i) & (RING - 1);
+      const double2 pa = R[0][ea], qa = R[1][ea];
+      const double r2a = fma(U0, pa.x, fma(U1, pa.y, fma(U2, qa.x, A + qa.y)));
+      const double sa = weight(r2a);
+      const double2 wa = R[2][ea], va = R[3][ea];
+      r0 = fma(wa.x, sa, r0);
+      x0 = fma(wa.y, sa, x0);
+      y0 = fma(va.x, sa, y0);
+      z0 = fma(va.y, sa, z0);
+      if (COUNT) {
+        const unsigned ia = live && r2a <= rad2;
+        npairs += ia;
+        nnode += ia * mult;
+      }
+    }
+    if (COUNT && lane == 0) nevals += (unsigned long long)k * (unsigned)npg;
+    head = (head + k) & (RING - 1);
+    count -= k;
+  };
+
+  const double cc[3] = {c0, c1, c2};
+  int ulo[3], uhi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    ulo[d] = bin_floor(G, d, cc[d] - reach);
+    uhi[d] = bin_floor(G, d, cc[d] + reach);
+    if (G.periodic[d]) {
+      ulo[d] -= 1;
+      uhi[d] += 1;
+    } else {
+      ulo[d] = max(ulo[d], 0);
+      uhi[d] = min(uhi[d], G.dims[d] - 1);
+    }
+  }
+  const double reach_c = reach * (1 + 1e-6);
+  const double reach_c2 = reach_c * reach_c;
+  const double2 *__restrict__ pay = reinterpret_cast<const double2 *>(P.payload);
+
+  for (int bz = ulo[2]; bz <= uhi[2]; ++bz) {
+    int wz = bz, qz = 0;
+    if (G.periodic[2]) { qz = floor_div(bz, G.dims[2]); wz = bz - qz * G.dims[2]; }
+    const double sz = qz * G.period[2] - c2;
+    double dz2;
+    {
+      const double blo = G.origin[2] + bz * G.w[2], bhi = blo + G.w[2];
+      const double e = fmax(0.0, fmax(blo - c2, c2 - bhi)) - G.slack[2];
+      dz2 = e > 0 ? e * e : 0.0;
+      if (dz2 > reach_c2) continue;
+    }
+    for (int by = ulo[1]; by <= uhi[1]; ++by) {
+      int wy = by, qy = 0;
+      if (G.periodic[1]) { qy = floor_div(by, G.dims[1]); wy = by - qy * G.dims[1]; }
+      const double sy = qy * G.period[1] - c1;
+      int bx0, bx1;
+      {
+        const double blo = G.origin[1] + by * G.w[1], bhi = blo + G.w[1];
+        const double e = fmax(0.0, fmax(blo - c1, c1 - bhi)) - G.slack[1];
+        const double dyz2 = dz2 + (e > 0 ? e * e : 0.0);
+        if (dyz2 > reach_c2) continue;
+        const double rem = sqrt(reach_c2 - dyz2);
+        bx0 = bin_floor(G, 0, c0 - rem);
+        bx1 = bin_floor(G, 0, c0 + rem);
+        if (G.periodic[0]) {
+          bx0 -= 1;
+          bx1 += 1;
+        }
+        bx0 = max(bx0, ulo[0]);
+        bx1 = min(bx1, uhi[0]);
+      }
+      int bx = bx0;
+      while (bx <= bx1) {
+        int wx = bx, qx = 0, seg_end = bx1;
+        if (G.periodic[0]) {
+          qx = floor_div(bx, G.dims[0]);
+          wx = bx - qx * G.dims[0];
+          seg_end = min(bx1, (qx + 1) * G.dims[0] - 1);
+        }
+        const double sx = qx * G.period[0] - c0;
+        const long long row = (long long)G.dims[0] * (wy + (long long)G.dims[1] * wz);
+        const uint32_t s0 = P.starts[row + wx];
+        const uint32_t s1 = P.starts[row + wx + (seg_end - bx) + 1];
+        bx = seg_end + 1;
+        for (uint32_t b0 = s0; b0 < s1; b0 += 32) {
+          const uint32_t k = b0 + lane;
+          bool in = false;
+          double w0 = 0, w1 = 0, w2 = 0, d2 = 0, qn = 0;
+          if (k < s1) {
+            const double2 xy = pay[4 * (size_t)k], zq = pay[4 * (size_t)k + 1];
+            w0 = xy.x + sx;
+            w1 = xy.y + sy;
+            w2 = zq.x + sz;
+            qn = zq.y;
+            d2 = w0 * w0 + w1 * w1 + w2 * w2;
+            in = d2 <= cull2;
+          }
+          const unsigned bal = __ballot_sync(0xffffffffu, in);
+          if (in) {
+            const double2 jv = pay[4 * (size_t)k + 2], jt = pay[4 * (size_t)k + 3];
+            const int slot = (head + count + __popc(bal & ((1u << lane) - 1u))) & (RING - 1);
+            R[0][slot] = make_double2(w0, w1);
+            R[1][slot] = make_double2(w2, d2);
+            R[2][slot] = make_double2(qn, jv.x);
+            R[3][slot] = make_double2(jv.y, jt.x);
+          }
+          count += __popc(bal);
+          __syncwarp();
+          if (count >= 32) {
+            drain(32);
+            __syncwarp();
+          }
+        }
+      }
+    }
+  }
+  if (count > 0) drain(count);
+  if (COUNT) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      npairs += __shfl_down_sync(0xffffffffu, npairs, o);
+      nnode += __shfl_down_sync(0xffffffffu, nnode, o);
+    }
+    if (lane == 0) {
+      if (npairs) atomicAdd(&counters[0], npairs);
+      if (nnode) atomicAdd(&counters[1], nnode);
+      if (nevals) atomicAdd(&counters[2], nevals);
+    }
+  }
+  if (live) {
+    const long long u = p0 + lane;
+    out[u] = r0 + r1;
+    out[npos + u] = x0 + x1;
+    out[2 * npos + u] = y0 + y1;
+    out[3 * npos + u] = z0 + z1;
+  }
+}
+
+// Every node takes the values of its position.
+__global__ void expand_kernel(long long nn, long long npos,
+                              const uint32_t *__restrict__ node_to_pos,
+                              const double *__restrict__ vals, double *__restrict__ rho,
+                              double *__restrict__ j) {
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  const uint32_t u = node_to_pos[n];
+  if (rho) rho[n] = vals[u];
+  if (j) {
+    j[n] = vals[npos + u];
+    j[nn + n] = vals[2 * npos + u];
+    j[2 * nn + n] = vals[3 * npos + u];
+  }
+}
+
+// Integration weight of a position: sum over its nodes of w_i |J_e| (the
+// normalising depositor's sum_e |J_e| sum_i w_i S_i, dep_normshape.hpp:155-164,
+// regrouped by position), in ascending node order.
+__global__ void position_weights_kernel(long long npos, const uint32_t *__restrict__ run_starts,
+                                        const uint32_t *__restrict__ run_nodes, int np,
+                                        const double *__restrict__ iw,
+                                        const double *__restrict__ jac,
+                                        double *__restrict__ W) {
+  long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (u >= npos) return;
+  double s = 0;
+  for (uint32_t k = run_starts[u]; k < run_starts[u + 1]; ++k) {
+    const uint32_t node = run_nodes[k];
+    s += iw[node % np] * jac[node / np];
+  }
+  W[u] = s;
+}
+
+struct TileBinsDev {
+  double origin[3], inv_w[3];
+  int dims[3];
+  const uint32_t *__restrict__ starts;
+  const uint32_t *__restrict__ tiles;
+};
+
+// Normalising pre-pass (dep_normshape.hpp:125-199): per particle the
+// integral of its deposited shape, sum_u W_u N S(x_u - x_p), over the
+// positions within the radius (one warp per particle, position tiles found
+// through uniform tile bins); scale = q / integral, or 0 with a warning for a
+// zero integral (the reference skips such a particle).
+template <bool ALPHA2>
+__global__ void normalize_kernel(DevMesh M, TileBinsDev TB, const double *__restrict__ pos,
+                                 long long npos, const double *__restrict__ boxes,
+                                 const double *__restrict__ W, ShapeParams S,
+                                 double normalizer, long long n,
+                                 const double *__restrict__ x, const double *__restrict__ q,
+                                 const uint32_t *__restrict__ el,
+                                 double *__restrict__ scale_out,
+                                 double *__restrict__ hits_out, DevStatus *st) {
+  const long long i = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  if (el && el[i] == PRT_INVALID) {
+    if (lane == 0) {
+      scale_out[i] = 0;
+      hits_out[i] = -1;
+    }
+    return;
+  }
+  const double px = x[i], py = x[n + i], pz = x[2 * n + i];
+  double integral = 0;
+  double hits = 0;
+  int lo_img[3], hi_img[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    lo_img[d] = hi_img[d] = 0;
+    if (M.pmin[d] != M.pmax[d]) {
+      const double pd = d == 0 ? px : (d == 1 ? py : pz);
+      if (pd - S.radius < M.pmin[d]) hi_img[d] = 1;
+      if (pd + S.radius > M.pmax[d]) lo_img[d] = -1;
+    }
+  }
+  for (int iz = lo_img[2]; iz <= hi_img[2]; ++iz)
+    for (int iy = lo_img[1]; iy <= hi_img[1]; ++iy)
+      for (int ix = lo_img[0]; ix <= hi_img[0]; ++ix) {
+        const double cc[3] = {px + ix * (M.pmax[0] - M.pmin[0]),
+                              py + iy * (M.pmax[1] - M.pmin[1]),
+                              pz + iz * (M.pmax[2] - M.pmin[2])};
+        int b0[3], b1[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double l = floor((cc[d] - S.radius - TB.origin[d]) * TB.inv_w[d]);
+          const double h = floor((cc[d] + S.radius - TB.origin[d]) * TB.inv_w[d]);
+          b0[d] = (int)fmax(0.0, fmin(l, TB.dims[d] - 1.0));
+          b1[d] = (int)fmax(0.0, fmin(h, TB.dims[d] - 1.0));
+        }
+        for (int bz = b0[2]; bz <= b1[2]; ++bz)
+          for (int by = b0[1]; by <= b1[1]; ++by)
+            for (int bx = b0[0]; bx <= b1[0]; ++bx) {
+              const long long bid = bx + (long long)TB.dims[0] * (by + (long long)TB.dims[1] * bz);
+              for (uint32_t k = TB.starts[bid]; k < TB.starts[bid + 1]; ++k) {
+                const uint32_t tile = TB.tiles[k];
+                const double *bx6 = boxes + 6 * (size_t)tile;
+                // a tile is visited in the first bin of the overlap of its
+                // bin range and the particle's bin range only
+                int first[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                  const double l = floor((bx6[d] - TB.origin[d]) * TB.inv_w[d]);
+                  first[d] = max((int)fmax(0.0, fmin(l, TB.dims[d] - 1.0)), b0[d]);
+                }
+                if (bx != first[0] || by != first[1] || bz != first[2]) continue;
+                double d2 = 0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                  const double e = fmax(0.0, fmax(bx6[d] - cc[d], cc[d] - bx6[3 + d]));
+                  d2 += e * e;
+                }
+                if (d2 > S.radius2) continue;
+                const long long p0 = (long long)tile * PRT_NODE_TILE;
+                const long long p1 = min(p0 + PRT_NODE_TILE, npos);
+                for (long long uu = p0 + lane; uu < p1; uu += 32) {
+                  const double e0 = pos[3 * uu] - cc[0], e1 = pos[3 * uu + 1] - cc[1],
+                               e2 = pos[3 * uu + 2] - cc[2];
+                  const double r2 = e0 * e0 + e1 * e1 + e2 * e2;
+                  if (r2 <= S.radius2) {
+                    const double rt = S.radius - r2 * S.inv_radius;
+                    const double s = normalizer * (ALPHA2 ? rt * rt : pow(rt, S.alpha));
+                    integral = fma(s, W[uu], integral);
+                    hits += 1;
+                  }
+                }
+              }
+            }
+      }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    integral += __shfl_xor_sync(0xffffffffu, integral, o);
+    hits += __shfl_xor_sync(0xffffffffu, hits, o);
+  }
+  if (lane == 0) {
+    if (integral == 0) {
+      scale_out[i] = 0;
+      record_warning(st, PRT_WARN_ZERO_MASS, i);
+    } else {
+      scale_out[i] = q[i] / integral;
+    }
+    hits_out[i] = hits;
+  }
+}
+
+// Deterministic single-block reduction of count / sum / sum of squares /
+// min / max of the applied scales (non-zero ones) and of the per-particle
+// position counts (live particles).
 __global__ void stats_kernel(long long n, const double *__restrict__ scale,
-                             const double *__restrict__ elc, double *__restrict__ out) {
-  // single block: deterministic tree reduction of count/sum/sumsq/min/max
+                             const double *__restrict__ hits, double *__restrict__ out) {
   __shared__ double sh[10][256];
   double acc[10] = {0, 0, 0, INFINITY, -INFINITY, 0, 0, 0, INFINITY, -INFINITY};
   for (long long i = threadIdx.x; i < n; i += blockDim.x) {
-    double c = elc[i];
-    if (c < 0) continue;  // dead particle
+    const double c = hits[i];
+    if (c < 0) continue;
     acc[5] += 1;
     acc[6] += c;
     acc[7] += c * c;
     acc[8] = fmin(acc[8], c);
     acc[9] = fmax(acc[9], c);
-    double s = scale[i];
-    if (s == 0) continue;  // zero-mass particle: skipped by the depositor
+    const double s = scale[i];
+    if (s == 0) continue;
     acc[0] += 1;
     acc[1] += s;
     acc[2] += s * s;
@@ -632,95 +576,188 @@ __global__ void stats_kernel(long long n, const double *__restrict__ scale,
   for (int o = 128; o > 0; o >>= 1) {
     if ((int)threadIdx.x < o)
       for (int k = 0; k < 10; ++k) {
-        double a = sh[k][threadIdx.x], b = sh[k][threadIdx.x + o];
-        sh[k][threadIdx.x] = (k == 3 || k == 8) ? fmin(a, b)
-                             : (k == 4 || k == 9) ? fmax(a, b)
-                                                  : a + b;
+        const double a = sh[k][threadIdx.x], b = sh[k][threadIdx.x + o];
+        sh[k][threadIdx.x] = (k == 3 || k == 8) ? fmin(a, b) : (k == 4 || k == 9) ? fmax(a, b) : a + b;
       }
     __syncthreads();
   }
   if (threadIdx.x < 10) out[threadIdx.x] = sh[threadIdx.x][0];
 }
 
+inline uint64_t spread_bits(uint64_t v) {  // 21 bits -> every third bit
+  v &= 0x1fffff;
+  v = (v | v << 32) & 0x1f00000000ffffull;
+  v = (v | v << 16) & 0x1f0000ff0000ffull;
+  v = (v | v << 8) & 0x100f00f00f00f00full;
+  v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+  v = (v | v << 2) & 0x1249249249249249ull;
+  return v;
+}
+
+template <class T>
+int upload_vec(const std::vector<T> &v, const T **dst) {
+  T *p = nullptr;
+  PRT_CHECK_CUDA(cudaMalloc(&p, std::max<size_t>(1, v.size()) * sizeof(T)));
+  if (!v.empty()) PRT_CHECK_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *dst = p;
+  return PRT_OK;
+}
+
 }  // namespace
 
-// ------------------------------------------------------------------ tiles
+// ------------------------------------------------------------ position set
 
-int prt_mesh_build_tiles(prt_mesh *m, const prt_mesh_desc *d) {
+int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
   const long long E = d->element_count;
   const int Np = d->nodes_per_element;
-  const int te = std::max(1, std::min(32, PRT_TILE_NODES / Np));
-  const long long tiles = (E + te - 1) / te;
-  std::vector<double> boxes(6 * (size_t)tiles), spheres(4 * (size_t)E);
+  const long long nn = E * (long long)Np;
+  const double *X = d->nodes;
   for (int a = 0; a < 3; ++a) {
     m->box_lo[a] = INFINITY;
     m->box_hi[a] = -INFINITY;
   }
-  for (long long e = 0; e < E; ++e) {
-    double c[3] = {0, 0, 0};
-    const double *xn = d->nodes + 3 * (size_t)e * Np;
-    for (int i = 0; i < Np; ++i)
-      for (int a = 0; a < 3; ++a) c[a] += xn[3 * i + a];
-    for (int a = 0; a < 3; ++a) c[a] /= Np;
-    double r2 = 0;
-    for (int i = 0; i < Np; ++i) {
-      double s = 0;
-      for (int a = 0; a < 3; ++a) s += (xn[3 * i + a] - c[a]) * (xn[3 * i + a] - c[a]);
-      r2 = std::max(r2, s);
+  for (long long i = 0; i < nn; ++i)
+    for (int a = 0; a < 3; ++a) {
+      m->box_lo[a] = std::min(m->box_lo[a], X[3 * i + a]);
+      m->box_hi[a] = std::max(m->box_hi[a], X[3 * i + a]);
     }
-    for (int a = 0; a < 3; ++a) spheres[4 * e + a] = c[a];
-    // a little slack so that rounding never culls a node inside the ball
-    spheres[4 * e + 3] = std::sqrt(r2) * (1 + 1e-9) + 1e-300;
-    const long long t = e / te;
-    double *b = &boxes[6 * t];
-    if (e % te == 0)
-      for (int a = 0; a < 3; ++a) {
-        b[a] = INFINITY;
-        b[3 + a] = -INFINITY;
-      }
-    for (int i = 0; i < Np; ++i)
-      for (int a = 0; a < 3; ++a) {
-        b[a] = std::min(b[a], xn[3 * i + a]);
-        b[3 + a] = std::max(b[3 + a], xn[3 * i + a]);
-        m->box_lo[a] = std::min(m->box_lo[a], xn[3 * i + a]);
-        m->box_hi[a] = std::max(m->box_hi[a], xn[3 * i + a]);
-      }
+  double ext = 0;
+  for (int a = 0; a < 3; ++a) ext = std::max(ext, m->box_hi[a] - m->box_lo[a]);
+  if (!(ext > 0)) ext = 1;
+  // Morton keys of the nodes quantised to 2^21 cells per axis
+  const double scale = (double)((1 << 21) - 1) / ext;
+  std::vector<uint64_t> key(nn);
+  for (long long i = 0; i < nn; ++i) {
+    uint64_t k = 0;
+    for (int a = 0; a < 3; ++a) {
+      double qv = std::floor((X[3 * i + a] - m->box_lo[a]) * scale);
+      qv = std::min(std::max(qv, 0.0), (double)((1 << 21) - 1));
+      k |= spread_bits((uint64_t)qv) << a;
+    }
+    key[i] = k;
   }
-  m->tile_elements = te;
-  m->tile_count = tiles;
-  double *db;
-  PRT_CHECK_CUDA(cudaMalloc(&db, boxes.size() * sizeof(double)));
-  PRT_CHECK_CUDA(cudaMemcpy(db, boxes.data(), boxes.size() * sizeof(double), cudaMemcpyHostToDevice));
-  m->tile_boxes = db;
-  PRT_CHECK_CUDA(cudaMalloc(&db, spheres.size() * sizeof(double)));
-  PRT_CHECK_CUDA(cudaMemcpy(db, spheres.data(), spheres.size() * sizeof(double), cudaMemcpyHostToDevice));
-  m->el_spheres = db;
+  std::vector<uint32_t> order(nn);
+  std::iota(order.begin(), order.end(), 0u);
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    return key[a] != key[b] ? key[a] < key[b] : a < b;
+  });
+  // coincident nodes: same cell and within 1e-9 of the mesh extent
+  const double tol2 = (1e-9 * ext) * (1e-9 * ext);
+  std::vector<uint32_t> run_starts, node_to_pos(nn);
+  std::vector<double> pos;
+  run_starts.reserve(nn / 3);
+  pos.reserve(nn);
+  long long npos = 0;
+  for (long long r = 0; r < nn; ++r) {
+    const uint32_t i = order[r];
+    bool same = false;
+    if (r > 0 && key[i] == key[order[r - 1]]) {
+      const double *p = &pos[3 * (npos - 1)];
+      double s = 0;
+      for (int a = 0; a < 3; ++a) s += (X[3 * i + a] - p[a]) * (X[3 * i + a] - p[a]);
+      same = s <= tol2;
+    }
+    if (!same) {
+      run_starts.push_back((uint32_t)r);
+      for (int a = 0; a < 3; ++a) pos.push_back(X[3 * i + a]);
+      ++npos;
+    }
+    node_to_pos[i] = (uint32_t)(npos - 1);
+  }
+  run_starts.push_back((uint32_t)nn);
+  PositionSet &P = m->positions;
+  P.count = npos;
+  int rc;
+  if ((rc = upload_vec(pos, &P.pos))) return rc;
+  if ((rc = upload_vec(node_to_pos, &P.node_to_pos))) return rc;
+  if ((rc = upload_vec(run_starts, &P.run_starts))) return rc;
+  if ((rc = upload_vec(order, &P.run_nodes))) return rc;
 
-  // tile bins for the normalising pre-pass: uniform bins of about one tile
-  double ext[3], mean[3] = {0, 0, 0};
-  for (long long t = 0; t < tiles; ++t)
-    for (int a = 0; a < 3; ++a) mean[a] += boxes[6 * t + 3 + a] - boxes[6 * t + a];
-  TileBinsHost &H = m->tile_bins;
+  // tiles of PRT_NODE_TILE consecutive positions with their bounding boxes
+  const long long tiles = (npos + PRT_NODE_TILE - 1) / PRT_NODE_TILE;
+  std::vector<double> boxes(6 * (size_t)tiles);
+  double mean_ext[3] = {0, 0, 0};
+  for (long long t = 0; t < tiles; ++t) {
+    double *b = &boxes[6 * t];
+    for (int a = 0; a < 3; ++a) {
+      b[a] = INFINITY;
+      b[3 + a] = -INFINITY;
+    }
+    for (long long p = t * PRT_NODE_TILE; p < std::min(npos, (t + 1) * PRT_NODE_TILE); ++p)
+      for (int a = 0; a < 3; ++a) {
+        b[a] = std::min(b[a], pos[3 * p + a]);
+        b[3 + a] = std::max(b[3 + a], pos[3 * p + a]);
+      }
+    for (int a = 0; a < 3; ++a) mean_ext[a] += b[3 + a] - b[a];
+  }
+  P.tiles = tiles;
+  if ((rc = upload_vec(boxes, &P.tile_boxes))) return rc;
+
+  // warp groups: runs of at most 32 positions, cut wherever the Morton cell
+  // of about PRT_GROUP_TARGET positions changes, so that no group straddles
+  // two cells (compact groups, tight spheres)
+  {
+    double vol = 1;
+    for (int a = 0; a < 3; ++a) vol *= std::max(m->box_hi[a] - m->box_lo[a], 1e-300);
+    const double side = std::cbrt(PRT_GROUP_TARGET * vol / std::max<long long>(1, npos));
+    int level = (int)std::lround(std::log2(ext / side));
+    level = std::min(std::max(level, 0), 21);
+    const int shift = 3 * (21 - level);
+    std::vector<uint32_t> gstart;
+    gstart.reserve(npos / 16 + 2);
+    uint64_t prev_cell = ~0ull;
+    for (long long u = 0; u < npos; ++u) {
+      const uint64_t cell = key[order[run_starts[u]]] >> shift;
+      if (u == 0 || cell != prev_cell || u - gstart.back() >= PRT_WARP_NODES)
+        gstart.push_back((uint32_t)u);
+      prev_cell = cell;
+    }
+    gstart.push_back((uint32_t)npos);
+    const long long groups = (long long)gstart.size() - 1;
+    std::vector<double> spheres(4 * (size_t)std::max<long long>(1, groups));
+    for (long long g = 0; g < groups; ++g) {
+      double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+      for (uint32_t p = gstart[g]; p < gstart[g + 1]; ++p)
+        for (int a = 0; a < 3; ++a) {
+          lo[a] = std::min(lo[a], pos[3 * p + a]);
+          hi[a] = std::max(hi[a], pos[3 * p + a]);
+        }
+      double c[3], r2 = 0;
+      for (int a = 0; a < 3; ++a) c[a] = 0.5 * (lo[a] + hi[a]);
+      for (uint32_t p = gstart[g]; p < gstart[g + 1]; ++p) {
+        double s = 0;
+        for (int a = 0; a < 3; ++a) s += (pos[3 * p + a] - c[a]) * (pos[3 * p + a] - c[a]);
+        r2 = std::max(r2, s);
+      }
+      for (int a = 0; a < 3; ++a) spheres[4 * g + a] = c[a];
+      spheres[4 * g + 3] = std::sqrt(r2) * (1 + 1e-9) + 1e-300;
+    }
+    P.groups = groups;
+    if ((rc = upload_vec(gstart, &P.group_starts))) return rc;
+    if ((rc = upload_vec(spheres, &P.group_spheres))) return rc;
+  }
+
+  // uniform bins of about one tile listing the tiles whose box meets them
+  TileBinsHost &H = P.bins;
   long long nb = 1;
   for (int a = 0; a < 3; ++a) {
-    mean[a] = std::max(mean[a] / tiles, 1e-300);
-    ext[a] = m->box_hi[a] - m->box_lo[a];
-    int dims = ext[a] > 0 ? (int)std::max(1.0, std::min(512.0, std::floor(ext[a] / mean[a]))) : 1;
+    const double me = std::max(mean_ext[a] / std::max<long long>(1, tiles), 1e-300);
+    const double e = m->box_hi[a] - m->box_lo[a];
+    const int dims = e > 0 ? (int)std::max(1.0, std::min(512.0, std::floor(e / me))) : 1;
     H.dims[a] = dims;
     H.origin[a] = m->box_lo[a];
-    H.inv_w[a] = ext[a] > 0 ? dims / ext[a] : 0.0;
+    H.inv_w[a] = e > 0 ? dims / e : 0.0;
     nb *= dims;
   }
-  std::vector<uint32_t> counts(nb + 1, 0);
   auto brange = [&](long long t, int a, int &b0, int &b1) {
-    double l = std::floor((boxes[6 * t + a] - H.origin[a]) * H.inv_w[a]);
-    double h = std::floor((boxes[6 * t + 3 + a] - H.origin[a]) * H.inv_w[a]);
+    const double l = std::floor((boxes[6 * t + a] - H.origin[a]) * H.inv_w[a]);
+    const double h = std::floor((boxes[6 * t + 3 + a] - H.origin[a]) * H.inv_w[a]);
     b0 = (int)std::max(0.0, std::min(l, H.dims[a] - 1.0));
     b1 = (int)std::max(0.0, std::min(h, H.dims[a] - 1.0));
   };
+  std::vector<uint32_t> counts(nb + 1, 0), list;
   for (int pass = 0; pass < 2; ++pass) {
     std::vector<uint32_t> fill;
-    std::vector<uint32_t> list;
     if (pass == 1) {
       for (long long b = 0; b < nb; ++b) counts[b + 1] += counts[b];
       list.resize(counts[nb]);
@@ -732,24 +769,16 @@ int prt_mesh_build_tiles(prt_mesh *m, const prt_mesh_desc *d) {
       for (int z = r0[2]; z <= r1[2]; ++z)
         for (int y = r0[1]; y <= r1[1]; ++y)
           for (int x = r0[0]; x <= r1[0]; ++x) {
-            long long b = x + (long long)H.dims[0] * (y + (long long)H.dims[1] * z);
+            const long long b = x + (long long)H.dims[0] * (y + (long long)H.dims[1] * z);
             if (pass == 0)
               ++counts[b + 1];
             else
               list[fill[b]++] = (uint32_t)t;
           }
     }
-    if (pass == 1) {
-      uint32_t *dp;
-      PRT_CHECK_CUDA(cudaMalloc(&dp, counts.size() * 4));
-      PRT_CHECK_CUDA(cudaMemcpy(dp, counts.data(), counts.size() * 4, cudaMemcpyHostToDevice));
-      H.starts = dp;
-      PRT_CHECK_CUDA(cudaMalloc(&dp, std::max<size_t>(1, list.size()) * 4));
-      if (!list.empty())
-        PRT_CHECK_CUDA(cudaMemcpy(dp, list.data(), list.size() * 4, cudaMemcpyHostToDevice));
-      H.tiles = dp;
-    }
   }
+  if ((rc = upload_vec(counts, &H.starts))) return rc;
+  if ((rc = upload_vec(list, &H.tiles))) return rc;
   return PRT_OK;
 }
 
@@ -768,6 +797,7 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
   if (n > 0 && (!x || !q || (j && !v))) return PRT_ERR_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;
   const long long nn = mesh->dev.E * (long long)mesh->dev.Np;
+  const PositionSet &PS = mesh->positions;
   if (stats) std::memset(stats, 0, sizeof(*stats));
   if (n == 0) {
     if (rho) PRT_CHECK_CUDA(cudaMemsetAsync(rho, 0, nn * sizeof(double), s));
@@ -782,41 +812,46 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
   for (int d = 0; d < 3; ++d) S.reach[d] = shape.radius;
   int rc;
   BinGrid G;
-  if (!choose_bins(mesh, shape.radius, G, &rc)) return rc;
+  if (!choose_bins(mesh, mesh->box_lo, mesh->box_hi, shape.radius * BIN_FRACTION, shape.radius, G, &rc))
+    return rc;
+  const bool a2 = shape.alpha == 2;
 
   const double *scale = nullptr;
-  double normalizer = shape.normalizer;
   if (mode == PRT_DEPOSIT_NORMALIZED) {
     double *sc = (double *)ws_buffer(ws, PRT_WS_DEP_SCALE, 2 * sizeof(double) * (size_t)n, &rc);
     if (!sc) return rc;
-    int rc2;
-    double *iwd = (double *)ws_buffer(ws, PRT_WS_DEP_STATS, sizeof(double) * (64 + mesh->dev.Np), &rc2);
-    if (!iwd) return rc2;
-    PRT_CHECK_CUDA(cudaMemcpyAsync(iwd + 16, iw, sizeof(double) * mesh->dev.Np,
+    double *aux = (double *)ws_buffer(ws, PRT_WS_DEP_STATS,
+                                      sizeof(double) * (64 + mesh->dev.Np + PS.count), &rc);
+    if (!aux) return rc;
+    double *iwd = aux + 16, *W = aux + 64 + mesh->dev.Np;
+    PRT_CHECK_CUDA(cudaMemcpyAsync(iwd, iw, sizeof(double) * mesh->dev.Np,
                                    cudaMemcpyHostToDevice, s));
-    TileBins TB;
+    position_weights_kernel<<<prt_grid_blocks(PS.count, 256), 256, 0, s>>>(
+        PS.count, PS.run_starts, PS.run_nodes, mesh->dev.Np, iwd, mesh->dev.jacobians, W);
+    PRT_CHECK_CUDA(cudaGetLastError());
+    TileBinsDev TB;
     for (int d = 0; d < 3; ++d) {
-      TB.origin[d] = mesh->tile_bins.origin[d];
-      TB.inv_w[d] = mesh->tile_bins.inv_w[d];
-      TB.dims[d] = mesh->tile_bins.dims[d];
+      TB.origin[d] = PS.bins.origin[d];
+      TB.inv_w[d] = PS.bins.inv_w[d];
+      TB.dims[d] = PS.bins.dims[d];
     }
-    TB.starts = mesh->tile_bins.starts;
-    TB.tiles = mesh->tile_bins.tiles;
+    TB.starts = PS.bins.starts;
+    TB.tiles = PS.bins.tiles;
     const long long threads = 32 * (long long)n;
-    if (shape.alpha == 2)
+    if (a2)
       normalize_kernel<true><<<prt_grid_blocks(threads, 128), 128, 0, s>>>(
-          mesh->dev, TB, mesh->tile_boxes, mesh->el_spheres, mesh->tile_elements, iwd + 16, S,
-          shape.normalizer, n, x, q, el, sc, sc + n, ws->status);
+          mesh->dev, TB, PS.pos, PS.count, PS.tile_boxes, W, S, shape.normalizer, n, x, q, el,
+          sc, sc + n, ws->status);
     else
       normalize_kernel<false><<<prt_grid_blocks(threads, 128), 128, 0, s>>>(
-          mesh->dev, TB, mesh->tile_boxes, mesh->el_spheres, mesh->tile_elements, iwd + 16, S,
-          shape.normalizer, n, x, q, el, sc, sc + n, ws->status);
+          mesh->dev, TB, PS.pos, PS.count, PS.tile_boxes, W, S, shape.normalizer, n, x, q, el,
+          sc, sc + n, ws->status);
     PRT_CHECK_CUDA(cudaGetLastError());
     if (stats) {
-      stats_kernel<<<1, 256, 0, s>>>(n, sc, sc + n, iwd);
+      stats_kernel<<<1, 256, 0, s>>>(n, sc, sc + n, aux);
       PRT_CHECK_CUDA(cudaGetLastError());
       double h[10];
-      PRT_CHECK_CUDA(cudaMemcpyAsync(h, iwd, sizeof(h), cudaMemcpyDeviceToHost, s));
+      PRT_CHECK_CUDA(cudaMemcpyAsync(h, aux, sizeof(h), cudaMemcpyDeviceToHost, s));
       PRT_CHECK_CUDA(cudaStreamSynchronize(s));
       stats->norm_count = h[0];
       stats->norm_sum = h[1];
@@ -835,339 +870,52 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
   DepParticles P;
   {
     ScopedTimer timer(ws, PRT_TIME_DEPOSIT_STAGE, s);
-    if ((rc = stage_particles(ws, G, n, x, q, v, el, scale, normalizer, nullptr, P, nullptr, s)))
+    if ((rc = stage_particles(ws, G, n, x, q, v, el, scale, shape.normalizer, nullptr, P, s)))
       return rc;
   }
   unsigned long long *counter = nullptr;
   if (stats) {
     counter = (unsigned long long *)ws_buffer(ws, PRT_WS_DEP_COUNT, 64, &rc);
     if (!counter) return rc;
-    PRT_CHECK_CUDA(cudaMemsetAsync(counter, 0, 8, s));
+    PRT_CHECK_CUDA(cudaMemsetAsync(counter, 0, 24, s));
   }
-  MeshTarget T;
-  T.nodes = mesh->dev.nodes;
-  T.boxes = mesh->tile_boxes;
-  T.spheres = mesh->el_spheres;
-  T.E = mesh->dev.E;
-  T.Np = mesh->dev.Np;
-  T.tile_elements = mesh->tile_elements;
-  T.node_count = nn;
-  const bool a2 = shape.alpha == 2;
+  double *vals = (double *)ws_buffer(ws, PRT_WS_DEP_VALUES, 4 * sizeof(double) * PS.count, &rc);
+  if (!vals) return rc;
   {
     ScopedTimer timer(ws, PRT_TIME_DEPOSIT_GATHER, s);
-    const unsigned nb = (unsigned)mesh->tile_count;
+    const unsigned nb = (unsigned)((PS.groups + WARPS - 1) / WARPS);
     if (counter) {
       if (a2)
-        gather_kernel<MeshTarget, W_SHAPE2, true><<<nb, BLOCK, 0, s>>>(T, G, P, S, rho, j, nn,
-                                                                       nullptr, counter);
+        deposit_groups_kernel<true, true><<<nb, BLOCK, 0, s>>>(
+            PS.pos, PS.groups, PS.group_starts, PS.group_spheres, PS.run_starts, G, P, S,
+            PS.count, vals, counter);
       else
-        gather_kernel<MeshTarget, W_SHAPE_POW, true><<<nb, BLOCK, 0, s>>>(T, G, P, S, rho, j,
-                                                                          nn, nullptr, counter);
+        deposit_groups_kernel<false, true><<<nb, BLOCK, 0, s>>>(
+            PS.pos, PS.groups, PS.group_starts, PS.group_spheres, PS.run_starts, G, P, S,
+            PS.count, vals, counter);
     } else if (a2) {
-      gather_kernel<MeshTarget, W_SHAPE2><<<nb, BLOCK, 0, s>>>(T, G, P, S, rho, j, nn, nullptr,
-                                                               nullptr);
+      deposit_groups_kernel<true, false><<<nb, BLOCK, 0, s>>>(
+          PS.pos, PS.groups, PS.group_starts, PS.group_spheres, PS.run_starts, G, P, S,
+          PS.count, vals, nullptr);
     } else {
-      gather_kernel<MeshTarget, W_SHAPE_POW><<<nb, BLOCK, 0, s>>>(T, G, P, S, rho, j, nn,
-                                                                  nullptr, nullptr);
+      deposit_groups_kernel<false, false><<<nb, BLOCK, 0, s>>>(
+          PS.pos, PS.groups, PS.group_starts, PS.group_spheres, PS.run_starts, G, P, S,
+          PS.count, vals, nullptr);
     }
+    PRT_CHECK_CUDA(cudaGetLastError());
+  }
+  if (rho || j) {
+    expand_kernel<<<prt_grid_blocks(nn, 256), 256, 0, s>>>(nn, PS.count, PS.node_to_pos, vals,
+                                                           rho, j);
     PRT_CHECK_CUDA(cudaGetLastError());
   }
   if (counter) {
-    unsigned long long h = 0;
-    PRT_CHECK_CUDA(cudaMemcpyAsync(&h, counter, 8, cudaMemcpyDeviceToHost, s));
+    unsigned long long h[3] = {0, 0, 0};
+    PRT_CHECK_CUDA(cudaMemcpyAsync(h, counter, 24, cudaMemcpyDeviceToHost, s));
     PRT_CHECK_CUDA(cudaStreamSynchronize(s));
-    stats->pair_count = (double)h;
-  }
-  return PRT_OK;
-}
-
-// ------------------------------------------------------------------- grid
-
-struct prt_grid {
-  const prt_mesh *mesh;
-  int brick_count;
-  int np;
-  std::vector<prt_brick> host_bricks;
-  prt_brick *bricks = nullptr;
-  long long *tile_starts = nullptr;
-  long long tiles = 0;
-  long long grid_nodes = 0;
-  long long eog_count = 0;
-  uint32_t *eog_elements = nullptr;
-  uint64_t *eog_starts = nullptr;
-  uint32_t *eog_nodes = nullptr;
-  double *eog_weights = nullptr;
-  uint64_t *eog_mstarts = nullptr;
-  double *eog_matrices = nullptr;
-  int max_points = 0;
-  long long avg_count = 0;
-  uint32_t *avg_starts = nullptr;
-  uint32_t *avg_nodes = nullptr;
-};
-
-extern "C" int prt_grid_create(const prt_mesh *mesh, const prt_grid_desc *d, prt_grid **out) {
-  if (!mesh || !d || !out || d->brick_count <= 0 || !d->bricks ||
-      d->nodes_per_element != mesh->dev.Np)
-    return PRT_ERR_INVALID_ARGUMENT;
-  prt_grid *g = new prt_grid();
-  g->mesh = mesh;
-  g->brick_count = d->brick_count;
-  g->np = d->nodes_per_element;
-  g->host_bricks.assign(d->bricks, d->bricks + d->brick_count);
-  std::vector<long long> ts(d->brick_count + 1, 0);
-  long long gn = 0;
-  for (int b = 0; b < d->brick_count; ++b) {
-    const prt_brick &B = d->bricks[b];
-    for (int a = 0; a < 3; ++a)
-      if (B.dims[a] <= 0 || !(B.stepwidths[a] > 0)) {
-        delete g;
-        return PRT_ERR_INVALID_ARGUMENT;
-      }
-    long long t = (long long)((B.dims[0] + 7) / 8) * ((B.dims[1] + 3) / 4) * ((B.dims[2] + 3) / 4);
-    ts[b + 1] = ts[b] + t;
-    gn = std::max(gn, B.start_index + (long long)B.dims[0] * B.dims[1] * B.dims[2]);
-  }
-  g->tiles = ts.back();
-  g->grid_nodes = gn;
-  auto up = [&](auto **dst, const auto *src, size_t cnt) -> int {
-    using T = std::remove_pointer_t<std::remove_reference_t<decltype(*dst)>>;
-    *dst = nullptr;
-    if (cnt == 0) return PRT_OK;
-    if (!src) return PRT_ERR_INVALID_ARGUMENT;
-    PRT_CHECK_CUDA(cudaMalloc((void **)dst, cnt * sizeof(T)));
-    PRT_CHECK_CUDA(cudaMemcpy((void *)*dst, src, cnt * sizeof(T), cudaMemcpyHostToDevice));
-    return PRT_OK;
-  };
-  int rc = up(&g->bricks, d->bricks, d->brick_count);
-  if (!rc) rc = up(&g->tile_starts, ts.data(), ts.size());
-  g->eog_count = d->eog_count;
-  if (d->eog_count > 0) {
-    // one element-on-grid per element: the remap owns its nodes
-    std::vector<char> seen(mesh->dev.E, 0);
-    for (long long e = 0; e < d->eog_count && !rc; ++e) {
-      uint32_t el = d->eog_elements[e];
-      if (el >= mesh->dev.E || seen[el]) rc = PRT_ERR_INVALID_ARGUMENT;
-      else seen[el] = 1;
-      g->max_points = std::max<int>(g->max_points, (int)(d->eog_starts[e + 1] - d->eog_starts[e]));
-      if (d->eog_matrix_starts[e + 1] - d->eog_matrix_starts[e] !=
-          (uint64_t)g->np * (d->eog_starts[e + 1] - d->eog_starts[e]))
-        rc = PRT_ERR_INVALID_ARGUMENT;
-    }
-    const size_t tot = d->eog_starts[d->eog_count];
-    const size_t mtot = d->eog_matrix_starts[d->eog_count];
-    if (!rc) rc = up(&g->eog_elements, d->eog_elements, d->eog_count);
-    if (!rc) rc = up(&g->eog_starts, d->eog_starts, d->eog_count + 1);
-    if (!rc) rc = up(&g->eog_nodes, d->eog_grid_nodes, tot);
-    if (!rc) rc = up(&g->eog_weights, d->eog_weights, tot);
-    if (!rc) rc = up(&g->eog_mstarts, d->eog_matrix_starts, d->eog_count + 1);
-    if (!rc) rc = up(&g->eog_matrices, d->eog_matrices, mtot);
-  }
-  g->avg_count = d->avg_group_count;
-  if (!rc && d->avg_group_count > 0) {
-    rc = up(&g->avg_starts, d->avg_group_starts, d->avg_group_count + 1);
-    if (!rc) rc = up(&g->avg_nodes, d->avg_group_nodes, d->avg_group_starts[d->avg_group_count]);
-  }
-  if (rc) {
-    prt_grid_destroy(g);
-    return rc;
-  }
-  *out = g;
-  return PRT_OK;
-}
-
-extern "C" int prt_grid_destroy(prt_grid *g) {
-  if (!g) return PRT_OK;
-  void *ptrs[] = {g->bricks, g->tile_starts, g->eog_elements, g->eog_starts, g->eog_nodes,
-                  g->eog_weights, g->eog_mstarts, g->eog_matrices, g->avg_starts, g->avg_nodes};
-  for (void *p : ptrs)
-    if (p) cudaFree(p);
-  delete g;
-  return PRT_OK;
-}
-
-__global__ void brick_tag_kernel(const prt_brick *__restrict__ bricks, int nb, long long n,
-                                 const double *__restrict__ x, const uint32_t *__restrict__ el,
-                                 uint32_t *__restrict__ tag) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  uint32_t t = 0xffffffffu;
-  if (!el || el[i] != PRT_INVALID) {
-    const double p[3] = {x[i], x[n + i], x[2 * n + i]};
-    for (int b = 0; b < nb && t == 0xffffffffu; ++b) {
-      bool in = true;
-      for (int d = 0; d < 3; ++d)
-        in = in && p[d] >= bricks[b].origin[d] &&
-             p[d] < bricks[b].origin[d] + bricks[b].dims[d] * bricks[b].stepwidths[d];
-      if (in) t = (uint32_t)b;
-    }
-  }
-  tag[i] = t;
-}
-
-extern "C" int prt_deposit_grid(const prt_grid *g, prt_workspace *ws, int32_t weights,
-                                prt_shape_function shape, int64_t n, const double *x,
-                                const double *q, const double *v, const uint32_t *el,
-                                double *grid_rho, double *grid_j, void *stream) {
-  if (!g || !ws || n < 0 || n >= (1ll << 31)) return PRT_ERR_INVALID_ARGUMENT;
-  if (weights != PRT_GRID_SHAPE && weights != PRT_GRID_TRILINEAR) return PRT_ERR_INVALID_ARGUMENT;
-  if (weights == PRT_GRID_SHAPE && !(shape.radius > 0)) return PRT_ERR_INVALID_ARGUMENT;
-  if (n > 0 && (!x || !q || (grid_j && !v))) return PRT_ERR_INVALID_ARGUMENT;
-  cudaStream_t s = (cudaStream_t)stream;
-  const long long G_n = g->grid_nodes;
-  if (n == 0) {
-    if (grid_rho) PRT_CHECK_CUDA(cudaMemsetAsync(grid_rho, 0, G_n * sizeof(double), s));
-    if (grid_j) PRT_CHECK_CUDA(cudaMemsetAsync(grid_j, 0, 3 * G_n * sizeof(double), s));
-    return PRT_OK;
-  }
-  ShapeParams S;
-  int rc;
-  BinGrid G;
-  double reach_bins;
-  const uint32_t *tag = nullptr;
-  double normalizer;
-  if (weights == PRT_GRID_SHAPE) {
-    S.radius = shape.radius;
-    S.radius2 = shape.radius * shape.radius;
-    S.inv_radius = 1.0 / shape.radius;
-    S.alpha = shape.alpha;
-    for (int d = 0; d < 3; ++d) S.reach[d] = shape.radius;
-    reach_bins = shape.radius;
-    normalizer = shape.normalizer;
-  } else {
-    // trilinear: a point receives from particles within one cell; the
-    // payload weight is q / dV (dV of the particle's brick, via the tag).
-    double hmax = 0;
-    for (const prt_brick &B : g->host_bricks)
-      for (int d = 0; d < 3; ++d) hmax = std::max(hmax, B.stepwidths[d]);
-    // a point receives from particles within one cell per axis, i.e. within
-    // sqrt(3) h: the cull sphere uses that radius
-    S.radius = hmax * std::sqrt(3.0) * (1 + 1e-12);
-    S.radius2 = S.radius * S.radius;
-    S.inv_radius = 1.0 / hmax;
-    S.alpha = 1;
-    for (int d = 0; d < 3; ++d) S.reach[d] = hmax;
-    reach_bins = hmax;
-    normalizer = 1.0;
-    if (g->brick_count > 1) {
-      // distinct cell volumes per brick are not supported in one payload
-      for (const prt_brick &B : g->host_bricks)
-        for (int d = 0; d < 3; ++d)
-          if (B.stepwidths[d] != g->host_bricks[0].stepwidths[d]) return PRT_ERR_INVALID_ARGUMENT;
-    }
-    const prt_brick &B0 = g->host_bricks[0];
-    normalizer = 1.0 / (B0.stepwidths[0] * B0.stepwidths[1] * B0.stepwidths[2]);
-    uint32_t *tg = (uint32_t *)ws_buffer(ws, PRT_WS_SORT_TMP, 4 * (size_t)n, &rc);
-    if (!tg) return rc;
-    brick_tag_kernel<<<prt_grid_blocks(n, 256), 256, 0, s>>>(g->bricks, g->brick_count, n, x, el, tg);
-    PRT_CHECK_CUDA(cudaGetLastError());
-    tag = tg;
-  }
-  // bins must cover the bricks as well as the mesh box
-  prt_mesh tmp = *g->mesh;
-  for (const prt_brick &B : g->host_bricks)
-    for (int d = 0; d < 3; ++d) {
-      tmp.box_lo[d] = std::min(tmp.box_lo[d], B.origin[d]);
-      tmp.box_hi[d] = std::max(tmp.box_hi[d], B.origin[d] + B.dims[d] * B.stepwidths[d]);
-    }
-  if (!choose_bins(&tmp, reach_bins, G, &rc)) return rc;
-  DepParticles P;
-  if ((rc = stage_particles(ws, G, n, x, q, v, el, nullptr, normalizer, tag, P, nullptr, s)))
-    return rc;
-  BrickTarget T;
-  T.bricks = g->bricks;
-  T.tile_starts = g->tile_starts;
-  T.brick_count = g->brick_count;
-  T.check_tag = weights == PRT_GRID_TRILINEAR;
-  if (grid_rho) PRT_CHECK_CUDA(cudaMemsetAsync(grid_rho, 0, G_n * sizeof(double), s));
-  if (grid_j) PRT_CHECK_CUDA(cudaMemsetAsync(grid_j, 0, 3 * G_n * sizeof(double), s));
-  if (weights == PRT_GRID_TRILINEAR)
-    gather_kernel<BrickTarget, W_TRILINEAR><<<(unsigned)g->tiles, BLOCK, 0, s>>>(
-        T, G, P, S, grid_rho, grid_j, G_n, g->bricks, nullptr);
-  else if (shape.alpha == 2)
-    gather_kernel<BrickTarget, W_SHAPE2><<<(unsigned)g->tiles, BLOCK, 0, s>>>(
-        T, G, P, S, grid_rho, grid_j, G_n, g->bricks, nullptr);
-  else
-    gather_kernel<BrickTarget, W_SHAPE_POW><<<(unsigned)g->tiles, BLOCK, 0, s>>>(
-        T, G, P, S, grid_rho, grid_j, G_n, g->bricks, nullptr);
-  PRT_CHECK_CUDA(cudaGetLastError());
-  return PRT_OK;
-}
-
-// Remap (dep_grid.hpp:270-358): one warp per element-on-grid; lanes own the
-// element's nodes, the weighted grid values are staged in shared memory.
-__global__ void remap_kernel(long long eog_count, int np, const uint32_t *__restrict__ els,
-                             const uint64_t *__restrict__ starts,
-                             const uint32_t *__restrict__ gnodes,
-                             const double *__restrict__ weights,
-                             const uint64_t *__restrict__ mstarts,
-                             const double *__restrict__ mats, const double *__restrict__ from,
-                             double *__restrict__ to, long long offset, long long inc) {
-  extern __shared__ double gv_all[];
-  const int warps = blockDim.x >> 5;
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long e = blockIdx.x * (long long)warps + wid;
-  if (e >= eog_count) return;
-  const uint64_t s = starts[e];
-  const int cnt = (int)(starts[e + 1] - s);
-  // stage at most 256 points per pass
-  double *gv = gv_all + wid * 256;
-  double acc[2] = {0, 0};
-  bool any = false;
-  const double *M = mats + mstarts[e];
-  for (int base = 0; base < cnt; base += 256) {
-    const int m = min(256, cnt - base);
-    for (int k = lane; k < m; k += 32) {
-      double w = weights[s + base + k] * from[offset + (long long)gnodes[s + base + k] * inc];
-      gv[k] = w;
-      any = any || w != 0;
-    }
-    __syncwarp();
-    for (int k = 0; k < m; ++k) {
-      const double g = gv[k];
-      for (int r = 0; r < 2; ++r) {
-        int i = lane + 32 * r;
-        if (i < np) acc[r] = fma(M[i + (size_t)np * (base + k)], g, acc[r]);
-      }
-    }
-    __syncwarp();
-  }
-  if (!__any_sync(0xffffffffu, any)) return;
-  double *y = to + (long long)els[e] * np * inc + offset;
-  for (int r = 0; r < 2; ++r) {
-    int i = lane + 32 * r;
-    if (i < np) y[i * inc] += acc[r];
-  }
-}
-
-__global__ void average_kernel(long long groups, const uint32_t *__restrict__ starts,
-                               const uint32_t *__restrict__ nodes, double *__restrict__ to,
-                               long long offset, long long inc) {
-  long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (gi >= groups) return;
-  uint32_t s = starts[gi], t = starts[gi + 1];
-  if (s == t) return;
-  double avg = 0;
-  for (uint32_t k = s; k < t; ++k) avg += to[offset + (long long)nodes[k] * inc];
-  avg /= (t - s);
-  for (uint32_t k = s; k < t; ++k) to[offset + (long long)nodes[k] * inc] = avg;
-}
-
-extern "C" int prt_remap_grid_to_mesh(const prt_grid *g, const double *from, double *to,
-                                      int64_t offset, int64_t inc, void *stream) {
-  if (!g || !from || !to || inc <= 0 || offset < 0 || g->np > 64) return PRT_ERR_INVALID_ARGUMENT;
-  cudaStream_t s = (cudaStream_t)stream;
-  if (g->eog_count > 0) {
-    const int warps = 4;
-    remap_kernel<<<prt_grid_blocks(g->eog_count, warps), 32 * warps,
-                   warps * 256 * sizeof(double), s>>>(
-        g->eog_count, g->np, g->eog_elements, g->eog_starts, g->eog_nodes, g->eog_weights,
-        g->eog_mstarts, g->eog_matrices, from, to, offset, inc);
-    PRT_CHECK_CUDA(cudaGetLastError());
-  }
-  if (g->avg_count > 0) {
-    average_kernel<<<prt_grid_blocks(g->avg_count, 128), 128, 0, s>>>(
-        g->avg_count, g->avg_starts, g->avg_nodes, to, offset, inc);
-    PRT_CHECK_CUDA(cudaGetLastError());
+    stats->pair_count = (double)h[0];
+    stats->node_pair_count = (double)h[1];
+    stats->evaluated_pairs = (double)h[2];
   }
   return PRT_OK;
 }

@@ -18,10 +18,11 @@ enum {
   PRT_WS_DEP_SCALE,
   PRT_WS_DEP_STATS,
   PRT_WS_DEP_COUNT,
+  PRT_WS_DEP_VALUES,
   PRT_WS_SLOTS
 };
 
-// Uniform bins over the mesh box listing the deposition tiles that overlap
+// Uniform bins over the mesh box listing the position tiles that overlap
 // each bin (used by the particle-centric normalising pass).
 struct TileBinsHost {
   double origin[3], inv_w[3];
@@ -30,18 +31,30 @@ struct TileBinsHost {
   const uint32_t *tiles = nullptr;
 };
 
+// Distinct node positions (coincident DG nodes merged), in Morton order:
+// the targets of the mesh deposition.
+struct PositionSet {
+  long long count = 0;
+  const double *pos = nullptr;            // [count][3]
+  const uint32_t *node_to_pos = nullptr;  // [Nn]
+  const uint32_t *run_starts = nullptr;   // [count + 1] into run_nodes
+  const uint32_t *run_nodes = nullptr;    // [Nn] node ids grouped by position, ascending
+  long long tiles = 0;                    // ceil(count / PRT_NODE_TILE)
+  const double *tile_boxes = nullptr;     // [tiles][6]: lo xyz, hi xyz
+  TileBinsHost bins;
+  // warp groups: runs of <= 32 consecutive positions that never straddle a
+  // Morton cell of about 24 positions, with their bounding spheres
+  long long groups = 0;
+  const uint32_t *group_starts = nullptr; // [groups + 1]
+  const double *group_spheres = nullptr;  // [groups][4]: centre xyz, radius
+};
+
 struct prt_mesh {
   DevMesh dev;
   const double *face_centroids = nullptr;  // [E][4][3]
   const double *face_radii = nullptr;      // [E][4]
-  // deposition tiles: consecutive elements grouped so that a tile holds at
-  // most PRT_TILE_NODES nodes; per tile the node bounding box
-  int tile_elements = 0;                   // elements per tile
-  long long tile_count = 0;
-  const double *tile_boxes = nullptr;      // [tiles][6]: lo xyz, hi xyz
-  const double *el_spheres = nullptr;      // [E][4]: node centroid xyz, radius
   double box_lo[3], box_hi[3];             // node bounding box of the mesh
-  TileBinsHost tile_bins;
+  PositionSet positions;
 };
 
 // CUDA-event timing of the main kernels (prt_workspace_timing).
@@ -79,7 +92,10 @@ struct prt_pusher {
   std::vector<double> w;  // [np][np], canonical monomial order
 };
 
-constexpr int PRT_TILE_NODES = 128;
+constexpr int PRT_NODE_TILE = 128;
+constexpr int PRT_WARP_NODES = 32;
+// target positions per Morton cell when cutting warp groups
+constexpr double PRT_GROUP_TARGET = 24.0;
 
 void *ws_buffer(prt_workspace *ws, int slot, size_t bytes, int *rc);
-int prt_mesh_build_tiles(prt_mesh *m, const prt_mesh_desc *d);
+int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d);

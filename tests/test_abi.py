@@ -37,7 +37,7 @@ def test_struct_layouts_match_header():
     assert C.sizeof(_lib.ShapeFunctionDesc) == 24
     assert C.sizeof(_lib.Brick) == 3 * 8 + 3 * 8 + 4 * 4 + 8
     assert C.sizeof(_lib.FindCounters) == 32
-    assert C.sizeof(_lib.DepositStats) == 11 * 8
+    assert C.sizeof(_lib.DepositStats) == 13 * 8
 
 
 def test_product_path_fails_loudly_without_a_gpu():
