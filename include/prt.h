@@ -249,6 +249,34 @@ int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
                       double *rho, double *j, int32_t precision,
                       prt_deposit_stats *stats, void *stream);
 
+/* Scratch capacity of prt_deposit_shape_noalloc, in bytes, per device. */
+#define PRT_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* No counterpart in the reference: the plain-form deposition of
+ * prt_deposit_shape (mode PRT_DEPOSIT_PLAIN, FP64) for callers that must not
+ * allocate device memory while they run -- code with a fixed, pre-reserved
+ * memory budget, real-time loops where an allocation would stall or
+ * synchronise the device, or hosts that forbid it. It calls no cudaMalloc,
+ * cudaFree or allocating library routine and takes no workspace: all scratch
+ * comes from one file-scope device array of PRT_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until exit. Inputs and outputs are the
+ * caller's, as for prt_deposit_shape; rho or j may be NULL.
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) and caches it; make that first call before any
+ *    stream capture.
+ *  - A call whose scratch (about 84 bytes per particle + 32 bytes per
+ *    distinct node position + bins + radix-sort storage) exceeds the
+ *    capacity returns PRT_ERR_CAPACITY before touching any pointer.
+ *  - All calls share the one array and each leaves its contents behind (no
+ *    region needs clearing: every one is written before it is read); calls
+ *    that overlap on the GPU (other streams, other host threads) race, so
+ *    serialise them. */
+int prt_deposit_shape_noalloc(const prt_mesh *mesh, prt_shape_function shape,
+                              int64_t n, const double *positions,
+                              const double *charges, const double *velocities,
+                              const uint32_t *elements, double *rho, double *j,
+                              void *stream);
+
 /* ------------------------------------------------------------ grid dep --- */
 
 /* One brick (grid.hpp:159-340): cell-centred points origin + (idx + 1/2) h,

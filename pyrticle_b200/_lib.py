@@ -27,6 +27,8 @@ ERRORS = {
     -6: "size exceeds the fixed scratch capacity",
 }
 PRT_WARN_ZERO_MASS = 1
+PRT_ERR_CAPACITY = -6
+NOALLOC_SCRATCH_BYTES = 64 << 20
 
 TIME_DEPOSIT_GATHER = 0
 TIME_DEPOSIT_STAGE = 1
@@ -140,6 +142,8 @@ SIGNATURES = {
                               C.POINTER(_vp), _d, _d, _d, _d, _i32, _vp]),
     "prt_deposit_shape": (_i32, [_vp, _vp, _i32, ShapeFunctionDesc, _dp, _i64, _vp, _vp,
                                  _vp, _vp, _vp, _vp, _i32, C.POINTER(DepositStats), _vp]),
+    "prt_deposit_shape_noalloc": (_i32, [_vp, ShapeFunctionDesc, _i64, _vp, _vp, _vp, _vp,
+                                         _vp, _vp, _vp]),
     "prt_grid_create": (_i32, [_vp, C.POINTER(GridDesc), C.POINTER(_vp)]),
     "prt_grid_destroy": (_i32, [_vp]),
     "prt_deposit_grid": (_i32, [_vp, _vp, _i32, ShapeFunctionDesc, _i64, _vp, _vp, _vp,

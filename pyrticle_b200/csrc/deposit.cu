@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -916,6 +917,134 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
     stats->pair_count = (double)h[0];
     stats->node_pair_count = (double)h[1];
     stats->evaluated_pairs = (double)h[2];
+  }
+  return PRT_OK;
+}
+
+// ---------------------------------------------- deposition without allocation
+//
+// Some callers cannot allocate device memory while they run: an application
+// that sizes and reserves all of its GPU memory up front (a fixed memory
+// budget, a pool handed to it by a host framework), a real-time loop where a
+// cudaMalloc would stall or synchronise the device, or code running where
+// allocating is not allowed at all. prt_deposit_shape grows workspace
+// buffers on demand, so it cannot serve them. prt_deposit_shape_noalloc runs
+// the same plain-form deposition with all of its scratch taken from one
+// fixed, file-scope device array instead.
+
+namespace {
+
+// The scratch: PRT_NOALLOC_SCRATCH_BYTES per device, held by every GPU that
+// loads this library until the process exits. Host code must not use the
+// symbol as an address (it is a host-side stand-in); it asks the runtime for
+// the device address once per device (noalloc_scratch_address).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[PRT_NOALLOC_SCRATCH_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+void *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+std::mutex g_noalloc_mutex;
+
+// Device address of the scratch for the current device; looked up with
+// cudaGetSymbolAddress on the first call per device and cached.
+int noalloc_scratch_address(void **out) {
+  int dev = 0;
+  PRT_CHECK_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return PRT_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    PRT_CHECK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    if (!p) return PRT_ERR_CUDA;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return PRT_OK;
+}
+
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" int prt_deposit_shape_noalloc(const prt_mesh *mesh, prt_shape_function shape,
+                                         int64_t n, const double *x, const double *q,
+                                         const double *v, const uint32_t *el, double *rho,
+                                         double *j, void *stream) {
+  if (!mesh || n < 0 || n >= (1ll << 31) || !(shape.radius > 0)) return PRT_ERR_INVALID_ARGUMENT;
+  const PositionSet &PS = mesh->positions;
+  const long long nn = mesh->dev.E * (long long)mesh->dev.Np;
+  int rc;
+  BinGrid G;
+  if (!choose_bins(mesh, mesh->box_lo, mesh->box_hi, shape.radius * BIN_FRACTION, shape.radius,
+                   G, &rc))
+    return rc;
+  // scratch layout: keys, sorted keys, values, sorted values, bin starts,
+  // packed particles, position sums, radix-sort temporary storage
+  size_t cub_bytes = 0;
+  int bits = 1;
+  while ((1ll << bits) <= G.nbins) ++bits;
+  PRT_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (uint32_t *)nullptr,
+                                                 (uint32_t *)nullptr, (uint32_t *)nullptr,
+                                                 (uint32_t *)nullptr, (int)std::max<int64_t>(n, 1),
+                                                 0, bits, (cudaStream_t)stream));
+  const size_t b_keys = align256(4 * (size_t)n);
+  const size_t b_starts = align256(4 * (size_t)(G.nbins + 2));
+  const size_t b_payload = align256(sizeof(double) * PAYLOAD * (size_t)n);
+  const size_t b_vals = align256(4 * sizeof(double) * (size_t)PS.count);
+  const size_t need = 4 * b_keys + b_starts + b_payload + b_vals + align256(cub_bytes);
+  if (need > (size_t)PRT_NOALLOC_SCRATCH_BYTES) return PRT_ERR_CAPACITY;
+  if (n > 0 && (!x || !q || (j && !v))) return PRT_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n == 0) {
+    if (rho) PRT_CHECK_CUDA(cudaMemsetAsync(rho, 0, nn * sizeof(double), s));
+    if (j) PRT_CHECK_CUDA(cudaMemsetAsync(j, 0, 3 * nn * sizeof(double), s));
+    return PRT_OK;
+  }
+  void *base = nullptr;
+  if ((rc = noalloc_scratch_address(&base))) return rc;
+  char *p = (char *)base;
+  uint32_t *keys = (uint32_t *)p;
+  uint32_t *keys_out = (uint32_t *)(p += b_keys);
+  uint32_t *vals = (uint32_t *)(p += b_keys);
+  uint32_t *vals_out = (uint32_t *)(p += b_keys);
+  uint32_t *starts = (uint32_t *)(p += b_keys);
+  double *payload = (double *)(p += b_starts);
+  double *posvals = (double *)(p += b_payload);
+  void *cub_temp = (void *)(p += b_vals);
+  // every region is fully written before it is read, so the contents left
+  // by an earlier call need no clearing
+  bin_keys_kernel<<<prt_grid_blocks(n, 256), 256, 0, s>>>(G, n, x, el, keys, vals);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  PRT_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(cub_temp, cub_bytes, keys, keys_out, vals,
+                                                 vals_out, (int)n, 0, bits, s));
+  bin_starts_kernel<<<prt_grid_blocks(G.nbins + 1, 256), 256, 0, s>>>(G.nbins, n, keys_out,
+                                                                      starts);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  payload_kernel<<<prt_grid_blocks(n, 256), 256, 0, s>>>(n, vals_out, x, q, v, nullptr,
+                                                         shape.normalizer, nullptr, payload);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  DepParticles P;
+  P.payload = payload;
+  P.starts = starts;
+  ShapeParams S;
+  S.radius = shape.radius;
+  S.radius2 = shape.radius * shape.radius;
+  S.inv_radius = 1.0 / shape.radius;
+  S.alpha = shape.alpha;
+  for (int d = 0; d < 3; ++d) S.reach[d] = shape.radius;
+  const unsigned nb = (unsigned)((PS.groups + WARPS - 1) / WARPS);
+  if (shape.alpha == 2)
+    deposit_groups_kernel<true, false><<<nb, BLOCK, 0, s>>>(
+        PS.pos, PS.groups, PS.group_starts, PS.group_spheres, PS.run_starts, G, P, S, PS.count,
+        posvals, nullptr);
+  else
+    deposit_groups_kernel<false, false><<<nb, BLOCK, 0, s>>>(
+        PS.pos, PS.groups, PS.group_starts, PS.group_spheres, PS.run_starts, G, P, S, PS.count,
+        posvals, nullptr);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  if (rho || j) {
+    expand_kernel<<<prt_grid_blocks(nn, 256), 256, 0, s>>>(nn, PS.count, PS.node_to_pos,
+                                                           posvals, rho, j);
+    PRT_CHECK_CUDA(cudaGetLastError());
   }
   return PRT_OK;
 }
