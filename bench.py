@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     return ap.parse_args()
 
 
@@ -271,6 +272,17 @@ def main():
             dist.all_reduce(j)
         return rho, j
 
+    def one_step_mixed():
+        m.depositor.precision = "mixed"
+        try:
+            rho, j = m.step(s, fields, w.dt, steps=1, check=False)
+        finally:
+            m.depositor.precision = "fp64"
+        if world > 1:
+            dist.all_reduce(rho)
+            dist.all_reduce(j)
+        return rho, j
+
     for _ in range(args.warmup):
         one_step()
     torch.cuda.synchronize()
@@ -305,6 +317,43 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
     value = world * n * args.steps / (ms * 1e-3)
+
+    # ---- the mixed-precision form on the same workload ----
+    mixed = None
+    if not args.no_mixed:
+        # accuracy: one deposition of the same store in both forms
+        r64, j64 = m.depositor.deposit_densities_device(s, precision="fp64")
+        r32, j32 = m.depositor.deposit_densities_device(s, precision="mixed")
+        err_rho = float(torch.linalg.norm(r32 - r64) / torch.linalg.norm(r64))
+        err_j = float(torch.linalg.norm(j32 - j64) / torch.linalg.norm(j64))
+        for _ in range(args.warmup):
+            one_step_mixed()
+        _lib.check(m.lib.prt_workspace_timing(m.workspace, 1))
+        timing_read(m, 0, reset=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record()
+        for _ in range(args.steps):
+            one_step_mixed()
+        g1.record()
+        torch.cuda.synchronize()
+        _lib.check(m.lib.prt_workspace_timing(m.workspace, 0))
+        mms = g0.elapsed_time(g1)
+        mg, mk = timing_read(m, 0)
+        t = torch.tensor([mms], device="cuda", dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        mms = float(t.item())
+        mixed = {"value": world * n * args.steps / (mms * 1e-3), "unit": METRIC,
+                 "ms_per_step": mms / args.steps,
+                 "deposit_ms_per_step": mg / args.steps,
+                 "speedup_vs_fp64": ms / mms,
+                 "rho_rel_l2_vs_fp64": err_rho, "j_rel_l2_vs_fp64": err_j,
+                 "form": "shape weights and 32-particle batch sums in FP32, FP64 "
+                         "per-node combine; push, interpolation and locate FP64"}
 
     # ---- end to end: host buffers through the same API ----
     e2e = None
@@ -399,6 +448,8 @@ def main():
                                3 * kernel["deposit_stage"][1] + 8 * kernel["sort"][1])
     if e2e:
         line["e2e"] = e2e
+    if mixed:
+        line["mixed"] = mixed
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds)
     print(json.dumps(line), flush=True)

@@ -207,6 +207,14 @@ typedef struct prt_shape_function {
   double normalizer;
 } prt_shape_function;
 
+/* Arithmetic of a call (`precision` arguments). */
+enum prt_precision {
+  PRT_PRECISION_FP64 = 0,  /* plain form: FP64 throughout */
+  /* chosen form: deposition weights and per-batch sums in FP32, combined
+   * into FP64 per node; positions, momenta and locate stay FP64 */
+  PRT_PRECISION_MIXED = 1
+};
+
 enum prt_deposit_mode {
   PRT_DEPOSIT_PLAIN = 0,      /* ShapeFunctionDepositor (dep_shape.hpp) */
   PRT_DEPOSIT_NORMALIZED = 1  /* NormalizedShapeFunctionDepositor (dep_normshape.hpp) */

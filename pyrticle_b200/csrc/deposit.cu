@@ -402,6 +402,194 @@ __global__ void __launch_bounds__(BLOCK, PRT_GATHER_MIN_BLOCKS)
   }
 }
 
+// Mixed-precision form of deposit_groups_kernel: the same culling and order,
+// with the particle-to-position geometry and the shape weight in FP32
+// (coordinates relative to the group centre, taken from the FP64 positions)
+// and the contributions summed in FP32 over each batch of 32 ring entries,
+// then combined into FP64 per-position accumulators. A ring entry is 32
+// bytes: (wx, wy, wz, |w|^2), (qN, qN vx, qN vy, qN vz).
+template <bool ALPHA2>
+__global__ void __launch_bounds__(BLOCK, PRT_GATHER_MIN_BLOCKS)
+    deposit_groups_mixed_kernel(const double *__restrict__ pos, long long ngroups,
+                                const uint32_t *__restrict__ gstarts,
+                                const double *__restrict__ gspheres, BinGrid G,
+                                DepParticles P, ShapeParams S, long long npos,
+                                double *__restrict__ out) {
+  __shared__ float4 ring[WARPS][2][RING];
+
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long g = blockIdx.x * (long long)WARPS + wid;
+  if (g >= ngroups) return;  // whole warp
+  const uint32_t p0 = gstarts[g];
+  const int npg = (int)(gstarts[g + 1] - p0);
+  const bool live = lane < npg;
+  float4(*R)[RING] = ring[wid];
+
+  const double c0 = gspheres[4 * g], c1 = gspheres[4 * g + 1], c2 = gspheres[4 * g + 2];
+  const double reach = S.radius + gspheres[4 * g + 3];
+  const double cull2 = (reach * (1 + 1e-9)) * (reach * (1 + 1e-9));
+  float U0 = 0, U1 = 0, U2 = 0, A = 0;
+  if (live) {
+    const long long u = p0 + lane;
+    const float u0 = (float)(pos[3 * u] - c0), u1 = (float)(pos[3 * u + 1] - c1),
+                u2 = (float)(pos[3 * u + 2] - c2);
+    A = u0 * u0 + u1 * u1 + u2 * u2;
+    U0 = -2 * u0;
+    U1 = -2 * u1;
+    U2 = -2 * u2;
+  }
+  double r64 = 0, x64 = 0, y64 = 0, z64 = 0;
+  const float neg_inv_a = (float)-S.inv_radius, rad = (float)S.radius, alpha = (float)S.alpha;
+  auto weight = [&](float r2) -> float {
+    const float tr = fmaf(r2, neg_inv_a, rad);
+    if (ALPHA2) {
+      const float tp = fmaxf(tr, 0.0f);
+      return tp * tp;
+    }
+    return tr > 0 ? powf(tr, alpha) : 0.0f;
+  };
+  int head = 0, count = 0;
+  auto drain = [&](int k) {
+    float ra = 0, xa = 0, ya = 0, za = 0, rb = 0, xb = 0, yb = 0, zb = 0;
+    int i = 0;
+    for (; i + 1 < k; i += 2) {
+      const int ea = (head + i) & (RING - 1), eb = (head + i + 1) & (RING - 1);
+      const float4 pa = R[0][ea], pb = R[0][eb];
+      const float r2a = fmaf(U0, pa.x, fmaf(U1, pa.y, fmaf(U2, pa.z, A + pa.w)));
+      const float r2b = fmaf(U0, pb.x, fmaf(U1, pb.y, fmaf(U2, pb.z, A + pb.w)));
+      const float sa = weight(r2a), sb = weight(r2b);
+      const float4 qa = R[1][ea], qb = R[1][eb];
+      ra = fmaf(qa.x, sa, ra);
+      xa = fmaf(qa.y, sa, xa);
+      ya = fmaf(qa.z, sa, ya);
+      za = fmaf(qa.w, sa, za);
+      rb = fmaf(qb.x, sb, rb);
+      xb = fmaf(qb.y, sb, xb);
+      yb = fmaf(qb.z, sb, yb);
+      zb = fmaf(qb.w, sb, zb);
+    }
+    if (i < k) {
+      const int ea = (head + i) & (RING - 1);
+      const float4 pa = R[0][ea];
+      const float r2a = fmaf(U0, pa.x, fmaf(U1, pa.y, fmaf(U2, pa.z, A + pa.w)));
+      const float sa = weight(r2a);
+      const float4 qa = R[1][ea];
+      ra = fmaf(qa.x, sa, ra);
+      xa = fmaf(qa.y, sa, xa);
+      ya = fmaf(qa.z, sa, ya);
+      za = fmaf(qa.w, sa, za);
+    }
+    r64 += (double)ra + (double)rb;
+    x64 += (double)xa + (double)xb;
+    y64 += (double)ya + (double)yb;
+    z64 += (double)za + (double)zb;
+    head = (head + k) & (RING - 1);
+    count -= k;
+  };
+
+  const double cc[3] = {c0, c1, c2};
+  int ulo[3], uhi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    ulo[d] = bin_floor(G, d, cc[d] - reach);
+    uhi[d] = bin_floor(G, d, cc[d] + reach);
+    if (G.periodic[d]) {
+      ulo[d] -= 1;
+      uhi[d] += 1;
+    } else {
+      ulo[d] = max(ulo[d], 0);
+      uhi[d] = min(uhi[d], G.dims[d] - 1);
+    }
+  }
+  const double reach_c = reach * (1 + 1e-6);
+  const double reach_c2 = reach_c * reach_c;
+  const double2 *__restrict__ pay = reinterpret_cast<const double2 *>(P.payload);
+
+  for (int bz = ulo[2]; bz <= uhi[2]; ++bz) {
+    int wz = bz, qz = 0;
+    if (G.periodic[2]) { qz = floor_div(bz, G.dims[2]); wz = bz - qz * G.dims[2]; }
+    const double sz = qz * G.period[2] - c2;
+    double dz2;
+    {
+      const double blo = G.origin[2] + bz * G.w[2], bhi = blo + G.w[2];
+      const double e = fmax(0.0, fmax(blo - c2, c2 - bhi)) - G.slack[2];
+      dz2 = e > 0 ? e * e : 0.0;
+      if (dz2 > reach_c2) continue;
+    }
+    for (int by = ulo[1]; by <= uhi[1]; ++by) {
+      int wy = by, qy = 0;
+      if (G.periodic[1]) { qy = floor_div(by, G.dims[1]); wy = by - qy * G.dims[1]; }
+      const double sy = qy * G.period[1] - c1;
+      int bx0, bx1;
+      {
+        const double blo = G.origin[1] + by * G.w[1], bhi = blo + G.w[1];
+        const double e = fmax(0.0, fmax(blo - c1, c1 - bhi)) - G.slack[1];
+        const double dyz2 = dz2 + (e > 0 ? e * e : 0.0);
+        if (dyz2 > reach_c2) continue;
+        const double rem = sqrt(reach_c2 - dyz2);
+        bx0 = bin_floor(G, 0, c0 - rem);
+        bx1 = bin_floor(G, 0, c0 + rem);
+        if (G.periodic[0]) {
+          bx0 -= 1;
+          bx1 += 1;
+        }
+        bx0 = max(bx0, ulo[0]);
+        bx1 = min(bx1, uhi[0]);
+      }
+      int bx = bx0;
+      while (bx <= bx1) {
+        int wx = bx, qx = 0, seg_end = bx1;
+        if (G.periodic[0]) {
+          qx = floor_div(bx, G.dims[0]);
+          wx = bx - qx * G.dims[0];
+          seg_end = min(bx1, (qx + 1) * G.dims[0] - 1);
+        }
+        const double sx = qx * G.period[0] - c0;
+        const long long row = (long long)G.dims[0] * (wy + (long long)G.dims[1] * wz);
+        const uint32_t s0 = P.starts[row + wx];
+        const uint32_t s1 = P.starts[row + wx + (seg_end - bx) + 1];
+        bx = seg_end + 1;
+        for (uint32_t b0 = s0; b0 < s1; b0 += 32) {
+          const uint32_t k = b0 + lane;
+          bool in = false;
+          double w0 = 0, w1 = 0, w2 = 0, d2 = 0, qn = 0;
+          if (k < s1) {
+            const double2 xy = pay[4 * (size_t)k], zq = pay[4 * (size_t)k + 1];
+            w0 = xy.x + sx;
+            w1 = xy.y + sy;
+            w2 = zq.x + sz;
+            qn = zq.y;
+            d2 = w0 * w0 + w1 * w1 + w2 * w2;
+            in = d2 <= cull2;
+          }
+          const unsigned bal = __ballot_sync(0xffffffffu, in);
+          if (in) {
+            const double2 jv = pay[4 * (size_t)k + 2], jt = pay[4 * (size_t)k + 3];
+            const int slot = (head + count + __popc(bal & ((1u << lane) - 1u))) & (RING - 1);
+            const float f0 = (float)w0, f1 = (float)w1, f2 = (float)w2;
+            R[0][slot] = make_float4(f0, f1, f2, f0 * f0 + f1 * f1 + f2 * f2);
+            R[1][slot] = make_float4((float)qn, (float)jv.x, (float)jv.y, (float)jt.x);
+          }
+          count += __popc(bal);
+          __syncwarp();
+          if (count >= 32) {
+            drain(32);
+            __syncwarp();
+          }
+        }
+      }
+    }
+  }
+  if (count > 0) drain(count);
+  if (live) {
+    const long long u = p0 + lane;
+    out[u] = r64;
+    out[npos + u] = x64;
+    out[2 * npos + u] = y64;
+    out[3 * npos + u] = z64;
+  }
+}
+
 // Every node takes the values of its position.
 __global__ void expand_kernel(long long nn, long long npos,
                               const uint32_t *__restrict__ node_to_pos,
@@ -791,7 +979,9 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
                                  const uint32_t *el, double *rho, double *j,
                                  int32_t precision, prt_deposit_stats *stats,
                                  void *stream) {
-  if (!mesh || !ws || n < 0 || n >= (1ll << 31) || precision != 0) return PRT_ERR_INVALID_ARGUMENT;
+  if (!mesh || !ws || n < 0 || n >= (1ll << 31)) return PRT_ERR_INVALID_ARGUMENT;
+  if (precision != PRT_PRECISION_FP64 && precision != PRT_PRECISION_MIXED)
+    return PRT_ERR_INVALID_ARGUMENT;
   if (!(shape.radius > 0) || (mode != PRT_DEPOSIT_PLAIN && mode != PRT_DEPOSIT_NORMALIZED))
     return PRT_ERR_INVALID_ARGUMENT;
   if (mode == PRT_DEPOSIT_NORMALIZED && !iw) return PRT_ERR_INVALID_ARGUMENT;
@@ -885,7 +1075,14 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
   {
     ScopedTimer timer(ws, PRT_TIME_DEPOSIT_GATHER, s);
     const unsigned nb = (unsigned)((PS.groups + WARPS - 1) / WARPS);
-    if (counter) {
+    if (precision == PRT_PRECISION_MIXED) {
+      if (a2)
+        deposit_groups_mixed_kernel<true><<<nb, BLOCK, 0, s>>>(
+            PS.pos, PS.groups, PS.group_starts, PS.group_spheres, G, P, S, PS.count, vals);
+      else
+        deposit_groups_mixed_kernel<false><<<nb, BLOCK, 0, s>>>(
+            PS.pos, PS.groups, PS.group_starts, PS.group_spheres, G, P, S, PS.count, vals);
+    } else if (counter) {
       if (a2)
         deposit_groups_kernel<true, true><<<nb, BLOCK, 0, s>>>(
             PS.pos, PS.groups, PS.group_starts, PS.group_spheres, PS.run_starts, G, P, S,

@@ -20,11 +20,24 @@ class NormalizationStats:
         self.el_per_particle_stats = StatsGatherer()
 
 
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
 class ShapeFunctionDepositor(Depositor):
-    """rho[n] = sum_p q_p S(x_n - x_p), j = sum_p q_p v_p S (dep_shape.hpp)."""
+    """rho[n] = sum_p q_p S(x_n - x_p), j = sum_p q_p v_p S (dep_shape.hpp).
+
+    ``precision="fp64"`` is the plain form; ``"mixed"`` evaluates the shape
+    weights and sums them in FP32 per batch of 32 particles, combining the
+    batches into FP64 per node (the normalising scale stays FP64)."""
 
     name = "Shape"
     mode = _lib.DEPOSIT_PLAIN
+
+    def __init__(self, precision="fp64"):
+        Depositor.__init__(self)
+        if precision not in PRECISIONS:
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.precision = precision
 
     def set_shape_function(self, state, sf):
         Depositor.set_shape_function(self, state, sf)
@@ -33,7 +46,8 @@ class ShapeFunctionDepositor(Depositor):
         sf = self.shape_function
         return _lib.ShapeFunctionDesc(sf.radius, sf.exponent, sf.normalizer)
 
-    def deposit_densities_device(self, state, rho=True, j=True, precision=0):
+    def deposit_densities_device(self, state, rho=True, j=True, precision=None):
+        precision = PRECISIONS[precision or self.precision]
         self.deposit_hook()
         m = self.method
         r, jj = self._outputs(state)

@@ -328,3 +328,31 @@ def test_grid_deposit_and_remap(setup, weights):
     if weights == "trilinear":
         dV = float(np.prod(dep.bricks[0].stepwidths))
         assert gro.sum() * dV == pytest.approx(float(s.charges.sum()), rel=1e-12)
+
+
+def test_mixed_precision_deposit_error_bounds():
+    """The chosen form: FP32 shape weights and batch sums, FP64 combine.
+    rho and j within 1e-5 relative L2 of the FP64 form (config2's bound), on a
+    config2-like case (order 3, radius 0.08 cm) at reduced size."""
+    w = problems.make("config2", scale=0.005, cubes=(16, 16, 64))
+    m = make_method(w)
+    m.depositor.set_shape_function(None, PolynomialShapeFunction(w.shape_radius, 3, 2))
+    s = make_state(m, w)
+    r64, j64 = m.depositor.deposit_densities_device(s, precision="fp64")
+    r32, j32 = m.depositor.deposit_densities_device(s, precision="mixed")
+    er = rel_l2(r32.cpu().numpy(), r64.cpu().numpy())
+    ej = rel_l2(j32.cpu().numpy(), j64.cpu().numpy())
+    assert er < 1e-5 and ej < 1e-5, (er, ej)
+    assert er > 0  # it really ran in reduced precision
+
+
+def test_mixed_precision_normalized_charge():
+    w = problems.make("config0", scale=0.2)
+    m = make_method(w, depositor=NormalizedShapeFunctionDepositor(precision="mixed"))
+    m.depositor.set_shape_function(None, PolynomialShapeFunction(w.shape_radius, 3, 2))
+    s = make_state(m, w)
+    rho, _ = m.deposit_densities(s)
+    iw = m.depositor.integral_weights
+    total = float((rho.reshape(-1, len(iw)) @ iw * w.mesh.jacobians).sum())
+    # FP32 batch sums: the deposited charge is exact to FP32 rounding
+    assert total == pytest.approx(float(w.charges.sum()), rel=1e-6)
