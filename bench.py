@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-scale", type=float, default=1.0,
+                    help="particle-count scale of the differentiable workload (1M electrons)")
     return ap.parse_args()
 
 
@@ -239,6 +242,83 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def adjoint_bench(torch, scale, hbm_gbs, reps=2, checkpoint_every=10):
+    """Differentiable workload (16x16x64 cubes, order 3, 1M electrons, 100
+    LSRK4 steps, checkpoint every 10): forward (push + final deposition) and
+    backward (deposition adjoint + recomputation + stage adjoints) times of
+    one autograd call, loss sum over nodes of (j - j_target)^2 with j_target
+    from a run with 5% higher Bz; gradients with respect to the initial
+    momenta and the (Bz, focusing gradient) scalars. The chosen form (FP32
+    deposition in the forward) against the FP64 check run."""
+    from pyrticle_b200 import _lib, problems
+    from pyrticle_b200.adjoint import DifferentiableTrajectory
+    w = problems.make("config3", scale=scale)
+    m, sf = build_method(w, torch)
+    dev = torch.device("cuda")
+    f64 = torch.float64
+    basis = torch.as_tensor(w.field_basis, dtype=f64, device=dev).contiguous()
+    theta = torch.as_tensor(w.theta, dtype=f64, device=dev)
+    q = torch.as_tensor(w.charges, dtype=f64, device=dev)
+    mass = torch.as_tensor(w.masses, dtype=f64, device=dev)
+    x0 = torch.as_tensor(w.positions.T.copy(), dtype=f64, device=dev).contiguous()
+    p0 = torch.as_tensor(w.momenta.T.copy(), dtype=f64, device=dev).contiguous()
+    trajs = {form: DifferentiableTrajectory(m, q, mass, w.dt, w.steps, checkpoint_every,
+                                            basis=basis, precision=form)
+             for form in ("mixed", "fp64")}
+    with torch.no_grad():
+        _, j_t = trajs["fp64"](x0, p0, theta * torch.tensor([1.05, 1.0], dtype=f64, device=dev))
+
+    def run(traj):
+        p = p0.clone().requires_grad_()
+        th = theta.clone().requires_grad_()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        rho, j = traj(x0, p, th)
+        L = ((j - j_t) ** 2).sum()
+        e[1].record()
+        L.backward()
+        e[2].record()
+        torch.cuda.synchronize()
+        return e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), p.grad, th.grad, float(L)
+
+    out = {}
+    for form in ("mixed", "fp64"):
+        run(trajs[form])  # warm-up
+        _lib.check(m.lib.prt_workspace_timing(m.workspace, 1))
+        for cat in (_lib.TIME_LSRK_STAGE, _lib.TIME_STAGE_ADJOINT, _lib.TIME_DEPOSIT_ADJOINT):
+            timing_read(m, cat, reset=True)
+        f = b = 0.0
+        for _ in range(reps):
+            fm, bm, gp, gth, L = run(trajs[form])
+            f += fm
+            b += bm
+        _lib.check(m.lib.prt_workspace_timing(m.workspace, 0))
+        adj_ms, adj_n = timing_read(m, _lib.TIME_STAGE_ADJOINT)
+        dep_ms, dep_n = timing_read(m, _lib.TIME_DEPOSIT_ADJOINT)
+        n = len(w.positions)
+        # per adjoint stage: read x, p (48 B), element (4), q, m (16), four
+        # adjoints (96); write four adjoints (96)
+        adj_gbs = 260.0 * n / (adj_ms / max(adj_n, 1) * 1e-3) / 1e9
+        out[form] = {"forward_ms": f / reps, "backward_ms": b / reps,
+                     "ratio_backward_over_forward": b / f, "loss": L,
+                     "grad_p0": gp, "grad_theta": gth,
+                     "stage_adjoint_kernel_ms": adj_ms / max(adj_n, 1),
+                     "stage_adjoint_gbs": adj_gbs, "stage_adjoint_frac_hbm": adj_gbs / hbm_gbs,
+                     "deposit_adjoint_ms": dep_ms / max(dep_n, 1)}
+    g32, g64 = out["mixed"].pop("grad_p0"), out["fp64"].pop("grad_p0")
+    t32, t64 = out["mixed"].pop("grad_theta"), out["fp64"].pop("grad_theta")
+    return {"workload": f"config3: {w.mesh.element_count} tets order {w.order}, "
+                        f"{len(w.positions)} electrons, {w.steps} LSRK4 steps, checkpoint "
+                        f"every {checkpoint_every} steps with recomputation",
+            "chosen_form": out["mixed"], "fp64_check_run": out["fp64"],
+            "grad_p0_rel_l2_mixed_vs_fp64": float(torch.linalg.norm(g32 - g64) /
+                                                  torch.linalg.norm(g64)),
+            "grad_theta_mixed": [float(v) for v in t32],
+            "grad_theta_fp64": [float(v) for v in t64],
+            "loss_rel_diff_mixed_vs_fp64": abs(out["mixed"]["loss"] - out["fp64"]["loss"]) /
+                                           abs(out["fp64"]["loss"])}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -410,7 +490,7 @@ def main():
     sms, sk = kernel["lsrk_stage"]
     stage_bytes = 216.0 * n
     stage_gbs = stage_bytes / (sms / max(sk, 1) * 1e-3) / 1e9
-    roofline = {"bound": "fp64", "kernel": "gather_kernel<MeshTarget> (deposition)",
+    roofline = {"bound": "fp64", "kernel": "deposit_groups_kernel (deposition)",
                 "achieved": achieved, "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
                 "traffic": None,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 pipe; "
@@ -450,6 +530,8 @@ def main():
         line["e2e"] = e2e
     if mixed:
         line["mixed"] = mixed
+    if not args.no_adjoint and world == 1:
+        line["adjoint"] = adjoint_bench(torch, args.adjoint_scale, peaks["hbm_gbs"])
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds)
     print(json.dumps(line), flush=True)

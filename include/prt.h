@@ -126,7 +126,9 @@ enum prt_timing_category {
   PRT_TIME_DEPOSIT_STAGE = 1,  /* particle binning, sort and packing */
   PRT_TIME_LSRK_STAGE = 2,     /* fused RK stage kernel */
   PRT_TIME_SORT = 3,           /* prt_sort_by_element */
-  PRT_TIME_CATEGORIES = 4
+  PRT_TIME_STAGE_ADJOINT = 4,  /* prt_lsrk_stage_adjoint kernel */
+  PRT_TIME_DEPOSIT_ADJOINT = 5,/* prt_deposit_shape_adjoint */
+  PRT_TIME_CATEGORIES = 6
 };
 int prt_workspace_timing(prt_workspace *ws, int32_t enable);
 int prt_workspace_timing_read(prt_workspace *ws, int32_t category,
@@ -345,6 +347,62 @@ int prt_deposit_grid(const prt_grid *grid, prt_workspace *ws, int32_t weights,
 int prt_remap_grid_to_mesh(const prt_grid *grid, const double *from,
                            double *to, int64_t offset, int64_t increment,
                            void *stream);
+
+/* ------------------------------------------------- adjoint (reverse mode) ---
+ * No reference counterpart: the reference computes no derivatives. These
+ * differentiate prt_lsrk_stage, prt_get_velocities and prt_deposit_shape
+ * (plain mode) exactly, with every stage's containing element held fixed.
+ * The caller records the stage inputs (prt_lsrk_stage_record) and runs the
+ * adjoints in reverse order; checkpointing is the caller's choice. */
+
+#define PRT_MAX_FIELD_BASIS 4
+
+/* prt_lsrk_stage writing the updated state to separate arrays: reads
+ * (x_in, p_in, el_in), writes (x_out, p_out, el_out) (dead particles are
+ * copied), updates kx, kp in place. Outputs must not alias the inputs. The
+ * arithmetic is prt_lsrk_stage's, so a recorded run is bitwise identical to
+ * an in-place one. */
+int prt_lsrk_stage_record(const prt_pusher *pusher, prt_workspace *ws, int64_t n,
+                          const double *x_in, const double *p_in,
+                          const uint32_t *el_in, double *x_out, double *p_out,
+                          uint32_t *el_out, const double *charges,
+                          const double *masses, double *kx, double *kp,
+                          const double *const fields[6], double rk_a, double rk_b,
+                          double dt, double vacuum_c, void *stream);
+
+/* Adjoint of one prt_lsrk_stage. positions, momenta, elements: the stage's
+ * INPUT state. lam_x, lam_p, lam_kx, lam_kp [3][n]: on entry the adjoints of
+ * the stage's outputs, on exit those of its inputs. grad_fields: NULL, or six
+ * device [Nn] arrays (entries may be NULL) that accumulate dL/d(nodal field)
+ * (FP64 atomics: the last bits depend on the summation order). nbasis <=
+ * PRT_MAX_FIELD_BASIS basis fields, basis[6*k + c] component c of field k
+ * (NULL = zero): grad_theta[k] (device) accumulates sum over particles of
+ * dL/dE . E_k + dL/dB . B_k in a fixed order (deterministic). */
+int prt_lsrk_stage_adjoint(const prt_pusher *pusher, prt_workspace *ws, int64_t n,
+                           const double *positions, const double *momenta,
+                           const uint32_t *elements, const double *charges,
+                           const double *masses, double *lam_x, double *lam_p,
+                           double *lam_kx, double *lam_kp,
+                           const double *const fields[6], double rk_a, double rk_b,
+                           double dt, double vacuum_c, double *const grad_fields[6],
+                           int32_t nbasis, const double *const *basis,
+                           double *grad_theta, void *stream);
+
+/* Adjoint of prt_get_velocities: lam_p += (dv/dp)^T lam_v. */
+int prt_velocities_adjoint(int64_t n, const double *momenta, const double *masses,
+                           double vacuum_c, const double *lam_v, double *lam_p,
+                           void *stream);
+
+/* Adjoint of prt_deposit_shape in PRT_DEPOSIT_PLAIN mode: given dL/drho [Nn]
+ * and dL/dj [3][Nn] (either may be NULL), accumulates dL/dx into lam_x [3][n]
+ * and dL/dv into lam_v [3][n] (may be NULL). One warp per particle gathers
+ * the node adjoints within its radius; deterministic. */
+int prt_deposit_shape_adjoint(const prt_mesh *mesh, prt_workspace *ws,
+                              prt_shape_function shape, int64_t n,
+                              const double *positions, const double *charges,
+                              const double *velocities, const uint32_t *elements,
+                              const double *grad_rho, const double *grad_j,
+                              double *lam_x, double *lam_v, void *stream);
 
 /* ---------------------------------------------------------------- misc --- */
 

@@ -34,6 +34,9 @@ TIME_DEPOSIT_GATHER = 0
 TIME_DEPOSIT_STAGE = 1
 TIME_LSRK_STAGE = 2
 TIME_SORT = 3
+TIME_STAGE_ADJOINT = 4
+TIME_DEPOSIT_ADJOINT = 5
+MAX_FIELD_BASIS = 4
 
 DEPOSIT_PLAIN = 0
 DEPOSIT_NORMALIZED = 1
@@ -150,6 +153,14 @@ SIGNATURES = {
                                 _vp, _vp, _vp, _vp]),
     "prt_remap_grid_to_mesh": (_i32, [_vp, _vp, _vp, _i64, _i64, _vp]),
     "prt_sort_by_element": (_i32, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "prt_lsrk_stage_record": (_i32, [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                     _vp, _vp, _vp, C.POINTER(_vp), _d, _d, _d, _d, _vp]),
+    "prt_lsrk_stage_adjoint": (_i32, [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                      _vp, _vp, C.POINTER(_vp), _d, _d, _d, _d,
+                                      C.POINTER(_vp), _i32, C.POINTER(_vp), _vp, _vp]),
+    "prt_velocities_adjoint": (_i32, [_i64, _vp, _vp, _d, _vp, _vp, _vp]),
+    "prt_deposit_shape_adjoint": (_i32, [_vp, _vp, ShapeFunctionDesc, _i64, _vp, _vp, _vp,
+                                         _vp, _vp, _vp, _vp, _vp, _vp]),
     "prt_version": (C.c_char_p, []),
 }
 

@@ -624,13 +624,6 @@ __global__ void position_weights_kernel(long long npos, const uint32_t *__restri
   W[u] = s;
 }
 
-struct TileBinsDev {
-  double origin[3], inv_w[3];
-  int dims[3];
-  const uint32_t *__restrict__ starts;
-  const uint32_t *__restrict__ tiles;
-};
-
 // Normalising pre-pass (dep_normshape.hpp:125-199): per particle the
 // integral of its deposited shape, sum_u W_u N S(x_u - x_p), over the
 // positions within the radius (one warp per particle, position tiles found
@@ -658,69 +651,14 @@ __global__ void normalize_kernel(DevMesh M, TileBinsDev TB, const double *__rest
   const double px = x[i], py = x[n + i], pz = x[2 * n + i];
   double integral = 0;
   double hits = 0;
-  int lo_img[3], hi_img[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    lo_img[d] = hi_img[d] = 0;
-    if (M.pmin[d] != M.pmax[d]) {
-      const double pd = d == 0 ? px : (d == 1 ? py : pz);
-      if (pd - S.radius < M.pmin[d]) hi_img[d] = 1;
-      if (pd + S.radius > M.pmax[d]) lo_img[d] = -1;
-    }
-  }
-  for (int iz = lo_img[2]; iz <= hi_img[2]; ++iz)
-    for (int iy = lo_img[1]; iy <= hi_img[1]; ++iy)
-      for (int ix = lo_img[0]; ix <= hi_img[0]; ++ix) {
-        const double cc[3] = {px + ix * (M.pmax[0] - M.pmin[0]),
-                              py + iy * (M.pmax[1] - M.pmin[1]),
-                              pz + iz * (M.pmax[2] - M.pmin[2])};
-        int b0[3], b1[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const double l = floor((cc[d] - S.radius - TB.origin[d]) * TB.inv_w[d]);
-          const double h = floor((cc[d] + S.radius - TB.origin[d]) * TB.inv_w[d]);
-          b0[d] = (int)fmax(0.0, fmin(l, TB.dims[d] - 1.0));
-          b1[d] = (int)fmax(0.0, fmin(h, TB.dims[d] - 1.0));
-        }
-        for (int bz = b0[2]; bz <= b1[2]; ++bz)
-          for (int by = b0[1]; by <= b1[1]; ++by)
-            for (int bx = b0[0]; bx <= b1[0]; ++bx) {
-              const long long bid = bx + (long long)TB.dims[0] * (by + (long long)TB.dims[1] * bz);
-              for (uint32_t k = TB.starts[bid]; k < TB.starts[bid + 1]; ++k) {
-                const uint32_t tile = TB.tiles[k];
-                const double *bx6 = boxes + 6 * (size_t)tile;
-                // a tile is visited in the first bin of the overlap of its
-                // bin range and the particle's bin range only
-                int first[3];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                  const double l = floor((bx6[d] - TB.origin[d]) * TB.inv_w[d]);
-                  first[d] = max((int)fmax(0.0, fmin(l, TB.dims[d] - 1.0)), b0[d]);
-                }
-                if (bx != first[0] || by != first[1] || bz != first[2]) continue;
-                double d2 = 0;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                  const double e = fmax(0.0, fmax(bx6[d] - cc[d], cc[d] - bx6[3 + d]));
-                  d2 += e * e;
-                }
-                if (d2 > S.radius2) continue;
-                const long long p0 = (long long)tile * PRT_NODE_TILE;
-                const long long p1 = min(p0 + PRT_NODE_TILE, npos);
-                for (long long uu = p0 + lane; uu < p1; uu += 32) {
-                  const double e0 = pos[3 * uu] - cc[0], e1 = pos[3 * uu + 1] - cc[1],
-                               e2 = pos[3 * uu + 2] - cc[2];
-                  const double r2 = e0 * e0 + e1 * e1 + e2 * e2;
-                  if (r2 <= S.radius2) {
-                    const double rt = S.radius - r2 * S.inv_radius;
-                    const double s = normalizer * (ALPHA2 ? rt * rt : pow(rt, S.alpha));
-                    integral = fma(s, W[uu], integral);
-                    hits += 1;
-                  }
-                }
-              }
-            }
-      }
+  visit_positions_in_reach(M, TB, pos, npos, boxes, S, px, py, pz, lane,
+                           [&](long long uu, double, double, double, double r2) {
+                             const double rt = S.radius - r2 * S.inv_radius;
+                             const double s =
+                                 normalizer * (ALPHA2 ? rt * rt : pow(rt, S.alpha));
+                             integral = fma(s, W[uu], integral);
+                             hits += 1;
+                           });
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     integral += __shfl_xor_sync(0xffffffffu, integral, o);

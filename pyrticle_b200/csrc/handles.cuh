@@ -19,6 +19,8 @@ enum {
   PRT_WS_DEP_STATS,
   PRT_WS_DEP_COUNT,
   PRT_WS_DEP_VALUES,
+  PRT_WS_ADJ_POSITIONS,
+  PRT_WS_ADJ_PARTIALS,
   PRT_WS_SLOTS
 };
 

@@ -9,7 +9,9 @@ Five workloads, all in SI units (metres), as the reference works in SI
 * ``config1`` -- 32x32x128 cubes, order 3, 4M electrons, static Bz plus 8
   seeded Fourier modes of E and B, 128x128x512 brick grid, 100 steps.
 * ``config2`` -- config1's mesh and fields, 16M electrons, shape radius 0.08 cm.
-* ``config3`` -- 16x16x64 cubes, order 3, 1M electrons, 100 steps.
+* ``config3`` -- 16x16x64 cubes, order 3, 1M electrons, 100 steps, the
+  focusing fields of config0 (gradients with respect to Bz and the focusing
+  gradient are the differentiable set-up's parameters).
 * ``config4`` -- 64x64x128 cubes, order 4, 64M electrons in a Gaussian bunch.
 
 ``scale`` shrinks the particle count (and, through ``cubes``, the mesh) for
@@ -44,6 +46,10 @@ class Workload:
     steps: int
     brick_dims: tuple | None = None
     nodes: np.ndarray | None = None
+    # fields = sum_k theta[k] * field_basis[k] where the workload defines a
+    # basis (the differentiable set-ups): [K, 6, Nn] and [K]
+    field_basis: np.ndarray | None = None
+    theta: np.ndarray | None = None
 
     @property
     def particle_count(self) -> int:
@@ -94,6 +100,13 @@ def focusing_fields(nodes, axis_xy, bz=0.1, grad=1e6):
     f[1] = -grad * (nodes[:, 1] - axis_xy[1])
     f[5] = bz
     return f
+
+
+def focusing_basis(nodes, axis_xy):
+    """Basis of the focusing set-up: unit uniform Bz, unit focusing gradient
+    (``focusing_fields(bz, grad) = bz * basis[0] + grad * basis[1]``)."""
+    return np.stack([focusing_fields(nodes, axis_xy, bz=1.0, grad=0.0),
+                     focusing_fields(nodes, axis_xy, bz=0.0, grad=1.0)])
 
 
 def fourier_fields(nodes, rng, bz=0.1, modes=8, amp=1e4, lam=(0.2 * CM, 2 * CM)):
@@ -158,7 +171,10 @@ def make(name: str, scale: float = 1.0, cubes=None, steps=None, seed=1) -> Workl
                       lo, hi)
     else:
         x, p = _beam(n, rng, 0.25 * CM, 0.5 * CM, 3.5 * CM, 2.0, axis_xy)
-    if name == "config0":
+    basis = theta = None
+    if name in ("config0", "config3"):
+        basis = focusing_basis(nodes, axis_xy)
+        theta = np.array([0.1, 1e6])
         fields = focusing_fields(nodes, axis_xy)
     else:
         fields = fourier_fields(nodes, np.random.default_rng(2))
@@ -168,7 +184,7 @@ def make(name: str, scale: float = 1.0, cubes=None, steps=None, seed=1) -> Workl
     return Workload(name=name, mesh=mesh, order=order, positions=x, momenta=p,
                     charges=q, masses=m, fields=fields, shape_radius=a,
                     dt=stable_dt(mesh), steps=steps or nsteps, brick_dims=brick,
-                    nodes=nodes)
+                    nodes=nodes, field_basis=basis, theta=theta)
 
 
 def node_count(order: int) -> int:
