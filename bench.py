@@ -242,14 +242,14 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def adjoint_bench(torch, scale, hbm_gbs, reps=2, checkpoint_every=10):
+def adjoint_bench(torch, scale, hbm_gbs, reps=3, checkpoint_every=10):
     """Differentiable workload (16x16x64 cubes, order 3, 1M electrons, 100
     LSRK4 steps, checkpoint every 10): forward (push + final deposition) and
     backward (deposition adjoint + recomputation + stage adjoints) times of
     one autograd call, loss sum over nodes of (j - j_target)^2 with j_target
     from a run with 5% higher Bz; gradients with respect to the initial
     momenta and the (Bz, focusing gradient) scalars. The chosen form (FP32
-    deposition in the forward) against the FP64 check run."""
+    deposition in the forward, its own target) against the FP64 check run."""
     from pyrticle_b200 import _lib, problems
     from pyrticle_b200.adjoint import DifferentiableTrajectory
     w = problems.make("config3", scale=scale)
@@ -265,33 +265,41 @@ def adjoint_bench(torch, scale, hbm_gbs, reps=2, checkpoint_every=10):
     trajs = {form: DifferentiableTrajectory(m, q, mass, w.dt, w.steps, checkpoint_every,
                                             basis=basis, precision=form)
              for form in ("mixed", "fp64")}
+    # targets from the same form (a run with 5% higher Bz)
+    j_t = {}
     with torch.no_grad():
-        _, j_t = trajs["fp64"](x0, p0, theta * torch.tensor([1.05, 1.0], dtype=f64, device=dev))
+        for form, traj in trajs.items():
+            _, j_t[form] = traj(x0, p0, theta * torch.tensor([1.05, 1.0], dtype=f64, device=dev))
 
-    def run(traj):
+    def run(traj, target):
         p = p0.clone().requires_grad_()
         th = theta.clone().requires_grad_()
         e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         e[0].record()
         rho, j = traj(x0, p, th)
-        L = ((j - j_t) ** 2).sum()
+        L = ((j - target) ** 2).sum()
         e[1].record()
         L.backward()
         e[2].record()
         torch.cuda.synchronize()
-        return e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), p.grad, th.grad, float(L)
+        return (e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), p.grad, th.grad,
+                float(L.detach()))
 
     out = {}
     for form in ("mixed", "fp64"):
-        run(trajs[form])  # warm-up
+        run(trajs[form], j_t[form])  # warm-up
+        f = b = 0.0
+        for _ in range(reps):
+            fm, bm, gp, gth, L = run(trajs[form], j_t[form])
+            f += fm
+            b += bm
+        # one more call with per-kernel events and the backward's phases
         _lib.check(m.lib.prt_workspace_timing(m.workspace, 1))
         for cat in (_lib.TIME_LSRK_STAGE, _lib.TIME_STAGE_ADJOINT, _lib.TIME_DEPOSIT_ADJOINT):
             timing_read(m, cat, reset=True)
-        f = b = 0.0
-        for _ in range(reps):
-            fm, bm, gp, gth, L = run(trajs[form])
-            f += fm
-            b += bm
+        trajs[form].time_phases = True
+        run(trajs[form], j_t[form])
+        trajs[form].time_phases = False
         _lib.check(m.lib.prt_workspace_timing(m.workspace, 0))
         adj_ms, adj_n = timing_read(m, _lib.TIME_STAGE_ADJOINT)
         dep_ms, dep_n = timing_read(m, _lib.TIME_DEPOSIT_ADJOINT)
@@ -304,7 +312,8 @@ def adjoint_bench(torch, scale, hbm_gbs, reps=2, checkpoint_every=10):
                      "grad_p0": gp, "grad_theta": gth,
                      "stage_adjoint_kernel_ms": adj_ms / max(adj_n, 1),
                      "stage_adjoint_gbs": adj_gbs, "stage_adjoint_frac_hbm": adj_gbs / hbm_gbs,
-                     "deposit_adjoint_ms": dep_ms / max(dep_n, 1)}
+                     "deposit_adjoint_ms": dep_ms / max(dep_n, 1),
+                     "backward_phases_ms": dict(trajs[form].phase_ms)}
     g32, g64 = out["mixed"].pop("grad_p0"), out["fp64"].pop("grad_p0")
     t32, t64 = out["mixed"].pop("grad_theta"), out["fp64"].pop("grad_theta")
     return {"workload": f"config3: {w.mesh.element_count} tets order {w.order}, "

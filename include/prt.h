@@ -370,8 +370,18 @@ int prt_lsrk_stage_record(const prt_pusher *pusher, prt_workspace *ws, int64_t n
                           const double *const fields[6], double rk_a, double rk_b,
                           double dt, double vacuum_c, void *stream);
 
+/* Per-element monomial coefficients of nodal fields: for each of `count`
+ * device [Nn] arrays fields[k] (NULL entries skipped), coefficients[k]
+ * [E][Np] with f(r) = sum_j c_j monomial_j(r) on each element (canonical
+ * monomial order). The stage adjoint takes its fields in this form. */
+int prt_fields_to_monomial(const prt_pusher *pusher, int32_t count,
+                           const double *const *fields, double *const *coefficients,
+                           void *stream);
+
 /* Adjoint of one prt_lsrk_stage. positions, momenta, elements: the stage's
- * INPUT state. lam_x, lam_p, lam_kx, lam_kp [3][n]: on entry the adjoints of
+ * INPUT state. field_coefficients[6] and the basis: monomial coefficients
+ * (prt_fields_to_monomial) of the stage's fields and of the basis fields.
+ * lam_x, lam_p, lam_kx, lam_kp [3][n]: on entry the adjoints of
  * the stage's outputs, on exit those of its inputs. grad_fields: NULL, or six
  * device [Nn] arrays (entries may be NULL) that accumulate dL/d(nodal field)
  * (FP64 atomics: the last bits depend on the summation order). nbasis <=
@@ -383,8 +393,9 @@ int prt_lsrk_stage_adjoint(const prt_pusher *pusher, prt_workspace *ws, int64_t 
                            const uint32_t *elements, const double *charges,
                            const double *masses, double *lam_x, double *lam_p,
                            double *lam_kx, double *lam_kp,
-                           const double *const fields[6], double rk_a, double rk_b,
-                           double dt, double vacuum_c, double *const grad_fields[6],
+                           const double *const field_coefficients[6], double rk_a,
+                           double rk_b, double dt, double vacuum_c,
+                           double *const grad_fields[6],
                            int32_t nbasis, const double *const *basis,
                            double *grad_theta, void *stream);
 
@@ -395,8 +406,9 @@ int prt_velocities_adjoint(int64_t n, const double *momenta, const double *masse
 
 /* Adjoint of prt_deposit_shape in PRT_DEPOSIT_PLAIN mode: given dL/drho [Nn]
  * and dL/dj [3][Nn] (either may be NULL), accumulates dL/dx into lam_x [3][n]
- * and dL/dv into lam_v [3][n] (may be NULL). One warp per particle gathers
- * the node adjoints within its radius; deterministic. */
+ * and dL/dv into lam_v [3][n] (may be NULL). One lane per particle gathers
+ * the node adjoints within its radius, deterministically; fastest with the
+ * particles sorted by element (a warp's 32 particles share candidates). */
 int prt_deposit_shape_adjoint(const prt_mesh *mesh, prt_workspace *ws,
                               prt_shape_function shape, int64_t n,
                               const double *positions, const double *charges,

@@ -159,6 +159,7 @@ SIGNATURES = {
                                       _vp, _vp, C.POINTER(_vp), _d, _d, _d, _d,
                                       C.POINTER(_vp), _i32, C.POINTER(_vp), _vp, _vp]),
     "prt_velocities_adjoint": (_i32, [_i64, _vp, _vp, _d, _vp, _vp, _vp]),
+    "prt_fields_to_monomial": (_i32, [_vp, _i32, C.POINTER(_vp), C.POINTER(_vp), _vp]),
     "prt_deposit_shape_adjoint": (_i32, [_vp, _vp, ShapeFunctionDesc, _i64, _vp, _vp, _vp,
                                          _vp, _vp, _vp, _vp, _vp, _vp]),
     "prt_version": (C.c_char_p, []),

@@ -20,7 +20,9 @@ device buffers and the autograd boundary.
 
 Particles are sorted by element at each checkpoint (the element-sorted order
 keeps the field gathers coherent); adjoints are carried across segments by
-the particle order stored with each checkpoint.
+the particle order stored with each checkpoint. The launches of a segment
+(recomputation and stage adjoints) are captured once into a CUDA graph and
+replayed for the other segments of the same length.
 """
 
 from __future__ import annotations
@@ -46,6 +48,16 @@ def _ptrs(tensors):
 def _field_components(f):
     """Six component tensors of a [6, Nn] field, None where identically zero."""
     return [f[k] if bool(torch.any(f[k] != 0)) else None for k in range(6)]
+
+
+def monomial_coefficients(method, comps):
+    """Per-element monomial coefficients ([Nn] -> [E * Np]) of nodal field
+    components (None stays None), the form the stage adjoint reads."""
+    out = [None if c is None else torch.empty_like(c) for c in comps]
+    _lib.check(method.lib.prt_fields_to_monomial(
+        method.pusher.handle, len(comps), _ptrs(comps), _ptrs(out),
+        C.c_void_p(stream_handle())), "prt_fields_to_monomial")
+    return out
 
 
 class DifferentiableTrajectory:
@@ -79,7 +91,14 @@ class DifferentiableTrajectory:
         self.precision = PRECISIONS[precision]
         self.c = method.units.VACUUM_LIGHT_SPEED()
         self.nn = len(method.discretization)
-        self.last_counts = {}
+        # replay each segment's recomputation and adjoint launches from a
+        # CUDA graph captured on the first full segment
+        self.use_graphs = True
+        # when True, backward_run records CUDA events between its phases
+        # (launching every segment eagerly) and leaves the elapsed
+        # milliseconds per phase in self.phase_ms
+        self.time_phases = False
+        self.phase_ms = {}
 
     def __call__(self, x0, p0, theta=None, fields=None):
         dev = x0.device
@@ -154,10 +173,18 @@ class DifferentiableTrajectory:
         saved = dict(final=(x, p, el, q, m, order, v), checkpoints=checkpoints)
         return rho, j, saved
 
+    def _mark(self, marks, name):
+        if self.time_phases:
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record()
+            marks.append((name, ev))
+
     def backward_run(self, saved, F, grho, gj, want_fields, want_theta):
         meth = self.method
         lib = self.lib
         s = C.c_void_p(stream_handle())
+        marks = []
+        self._mark(marks, "start")
         x, p, el, q, m, order, v = saved["final"]
         n = x.shape[1]
         dev = x.device
@@ -175,17 +202,21 @@ class DifferentiableTrajectory:
         _lib.check(lib.prt_velocities_adjoint(n, p.data_ptr(), m.data_ptr(), self.c,
                                               lam_v.data_ptr(), lam_p.data_ptr(), s),
                    "prt_velocities_adjoint")
+        self._mark(marks, "deposit_adjoint")
         lam_kx = torch.zeros_like(x)
         lam_kp = torch.zeros_like(p)
         comps = _field_components(F)
         Fp = _ptrs(comps)
+        fcoef = monomial_coefficients(meth, comps)  # kept alive: Cp points into it
+        Cp = _ptrs(fcoef)
         nb = self.basis.shape[0] if (self.basis is not None and want_theta) else 0
         grad_theta = torch.zeros((max(nb, 1),), dtype=F64, device=dev)
         if nb:
             bcomps = []
             for k in range(nb):
                 bcomps += _field_components(self.basis[k])
-            Bp = _ptrs(bcomps)
+            bcoef = monomial_coefficients(meth, bcomps)  # kept alive: Bp points into it
+            Bp = _ptrs(bcoef)
         else:
             Bp = None
         grad_fields = torch.zeros((6, self.nn), dtype=F64, device=dev) if want_fields else None
@@ -193,7 +224,43 @@ class DifferentiableTrajectory:
 
         cps = saved["checkpoints"]
         cur_order = order
-        tape = None
+        Tmax = 5 * min(self.K, self.steps) if self.steps else 0
+        tx = torch.empty((Tmax + 1, 3, n), dtype=F64, device=dev)
+        tp = torch.empty((Tmax + 1, 3, n), dtype=F64, device=dev)
+        te = torch.empty((Tmax + 1, n), dtype=torch.int32, device=dev)
+        kx = torch.empty_like(x)
+        kp = torch.empty_like(p)
+        qs = torch.empty_like(self.q)
+        ms = torch.empty_like(self.m)
+        gth_ptr = grad_theta.data_ptr() if nb else None
+        ptr = lambda t: t.data_ptr()  # noqa: E731
+        # launch arguments of every stage of a segment, built once
+        rec_args = [(meth.pusher.handle, meth.workspace, n, ptr(tx[t]), ptr(tp[t]), ptr(te[t]),
+                     ptr(tx[t + 1]), ptr(tp[t + 1]), ptr(te[t + 1]), ptr(qs), ptr(ms), ptr(kx),
+                     ptr(kp), Fp, LSRK4_A[t % 5], LSRK4_B[t % 5], self.dt, self.c)
+                    for t in range(Tmax)]
+        adj_args = [(meth.pusher.handle, meth.workspace, n, ptr(tx[t]), ptr(tp[t]), ptr(te[t]),
+                     ptr(qs), ptr(ms), ptr(lam_x), ptr(lam_p), ptr(lam_kx), ptr(lam_kp), Cp,
+                     LSRK4_A[t % 5], LSRK4_B[t % 5], self.dt, self.c, Gp, nb, Bp, gth_ptr)
+                    for t in range(Tmax)]
+
+        def segment(T):
+            """Recompute T stages from tape slot 0, recording their inputs,
+            then run the T stage adjoints in reverse, on the current stream
+            (the capture stream while a graph is being captured)."""
+            cs = C.c_void_p(stream_handle())
+            kx.zero_()
+            kp.zero_()
+            for t in range(T):
+                _lib.check(lib.prt_lsrk_stage_record(*rec_args[t], cs), "prt_lsrk_stage_record")
+            self._mark(marks, "recompute")
+            for t in reversed(range(T)):
+                _lib.check(lib.prt_lsrk_stage_adjoint(*adj_args[t], cs),
+                           "prt_lsrk_stage_adjoint")
+            self._mark(marks, "stage_adjoint")
+
+        graphs = {}
+        self._mark(marks, "setup")
         for seg in reversed(range(len(cps))):
             xs, ps, els, order_s = cps[seg]
             if cur_order is not order_s:
@@ -201,49 +268,41 @@ class DifferentiableTrajectory:
                 inv = torch.empty_like(cur_order)
                 inv[cur_order] = torch.arange(n, dtype=torch.int64, device=dev)
                 idx = inv[order_s]
-                lam_x = lam_x[:, idx].contiguous()
-                lam_p = lam_p[:, idx].contiguous()
+                lam_x.copy_(lam_x[:, idx])
+                lam_p.copy_(lam_p[:, idx])
                 lam_kx.zero_()  # the first stage's a = 0 clears them at step boundaries
                 lam_kp.zero_()
-            qs = self.q[order_s].contiguous()
-            ms = self.m[order_s].contiguous()
-            nsteps = min(self.K, self.steps - seg * self.K)
-            T = 5 * nsteps
+            cur_order = order_s
+            T = 5 * min(self.K, self.steps - seg * self.K)
             if T == 0:
-                cur_order = order_s
                 continue
-            if tape is None or tape[0].shape[0] < T + 1:
-                tape = (torch.empty((T + 1, 3, n), dtype=F64, device=dev),
-                        torch.empty((T + 1, 3, n), dtype=F64, device=dev),
-                        torch.empty((T + 1, n), dtype=torch.int32, device=dev))
-            tx, tp, te = tape
+            torch.index_select(self.q, 0, order_s, out=qs)
+            torch.index_select(self.m, 0, order_s, out=ms)
             tx[0].copy_(xs)
             tp[0].copy_(ps)
             te[0].copy_(els)
-            kx = torch.zeros_like(xs)
-            kp = torch.zeros_like(ps)
-            for t in range(T):
-                a, b = LSRK4_A[t % 5], LSRK4_B[t % 5]
-                _lib.check(lib.prt_lsrk_stage_record(
-                    meth.pusher.handle, meth.workspace, n, tx[t].data_ptr(), tp[t].data_ptr(),
-                    te[t].data_ptr(), tx[t + 1].data_ptr(), tp[t + 1].data_ptr(),
-                    te[t + 1].data_ptr(), qs.data_ptr(), ms.data_ptr(), kx.data_ptr(),
-                    kp.data_ptr(), Fp, a, b, self.dt, self.c, s), "prt_lsrk_stage_record")
-            for t in reversed(range(T)):
-                a, b = LSRK4_A[t % 5], LSRK4_B[t % 5]
-                _lib.check(lib.prt_lsrk_stage_adjoint(
-                    meth.pusher.handle, meth.workspace, n, tx[t].data_ptr(), tp[t].data_ptr(),
-                    te[t].data_ptr(), qs.data_ptr(), ms.data_ptr(), lam_x.data_ptr(),
-                    lam_p.data_ptr(), lam_kx.data_ptr(), lam_kp.data_ptr(), Fp, a, b, self.dt,
-                    self.c, Gp, nb, Bp, grad_theta.data_ptr() if nb else None, s),
-                    "prt_lsrk_stage_adjoint")
-            self.last_tape_end = (tx[T], tp[T], te[T])
-            cur_order = order_s
+            self._mark(marks, "carry")
+            if not self.use_graphs or self.time_phases or seg == len(cps) - 1:
+                segment(T)  # eager (the first one also sizes libprt's scratch)
+                continue
+            g = graphs.get(T)
+            if g is None:
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    segment(T)
+                graphs[T] = g
+            g.replay()
         meth.check_status()
         inv = torch.empty_like(cur_order)
         inv[cur_order] = torch.arange(n, dtype=torch.int64, device=dev)
         gx0 = lam_x[:, inv].contiguous()
         gp0 = lam_p[:, inv].contiguous()
+        self._mark(marks, "carry")
+        if self.time_phases:
+            torch.cuda.synchronize()
+            self.phase_ms = {}
+            for (_, e0), (name, e1) in zip(marks[:-1], marks[1:]):
+                self.phase_ms[name] = self.phase_ms.get(name, 0.0) + e0.elapsed_time(e1)
         return gx0, gp0, (grad_theta[:nb] if nb else None), grad_fields
 
 

@@ -9,8 +9,8 @@
 //
 // Gather and scatter swap roles: the forward deposition gathers particles
 // onto node positions, its adjoint gathers node adjoints onto particles
-// (particle-centric, one warp per particle); the forward interpolation
-// gathers nodal fields onto particles, its adjoint scatters particle
+// (one lane per particle, position groups staged per warp); the forward
+// interpolation gathers nodal fields onto particles, its adjoint scatters particle
 // adjoints onto the nodes (warp-segmented sums, then FP64 atomics, only when
 // nodal field gradients are requested). Gradients along a few basis fields
 // (field = sum_k theta_k basis_k + fixed) are reduced per block in a fixed
@@ -42,6 +42,13 @@ struct GradFields {
 };
 
 constexpr int ADJ_BLOCK = 128;
+// resident blocks per SM the stage adjoint is compiled for: the kernel is
+// latency-bound, and 6 (80 registers at order 3, a few spilled) measured
+// fastest on B200 (0.25 ms per 1M-particle stage against 0.27 at 5 and 0.37
+// at 3); order 4 keeps 3 (35 monomials in registers)
+#ifndef ADJ_MIN_BLOCKS
+#define ADJ_MIN_BLOCKS 6
+#endif
 
 // Forward stage writing its output state to separate arrays (the recorded
 // tape keeps the input). Same arithmetic as lsrk_stage_kernel.
@@ -80,6 +87,26 @@ __global__ void __launch_bounds__(256, ORDER >= 4 ? 2 : 3)
   flush_counters(st, ctr);
 }
 
+// Per-element monomial coefficients of a nodal field:
+// f(r) = sum_n F_n l_n(r) = sum_j (sum_n F_n W[n][j]) m_j(r).
+template <int ORDER>
+__global__ void to_monomial_kernel(const Lagrange<ORDER> L, long long E,
+                                   const double *__restrict__ f, double *__restrict__ c) {
+  constexpr int NP = Lagrange<ORDER>::NP;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  double fv[NP];
+#pragma unroll
+  for (int nd = 0; nd < NP; ++nd) fv[nd] = f[e * NP + nd];
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    double s = 0;
+#pragma unroll
+    for (int nd = 0; nd < NP; ++nd) s = fma(L.w[nd * NP + j], fv[nd], s);
+    c[e * NP + j] = s;
+  }
+}
+
 __device__ __forceinline__ void cross3(const double a[3], const double b[3], double o[3]) {
   o[0] = a[1] * b[2] - a[2] * b[1];
   o[1] = a[2] * b[0] - a[0] * b[2];
@@ -88,11 +115,14 @@ __device__ __forceinline__ void cross3(const double a[3], const double b[3], dou
 
 // Adjoint of one stage (see the file comment). One thread per particle; dead
 // particles (PRT_INVALID) pass their adjoints through unchanged, as the
-// forward stage leaves them untouched. NODAL: also scatter dL/dfield onto the
-// nodes (per-warp shared staging of the Lagrange values and gE/gB, summed
-// over runs of lanes in one element, then one atomic per run and node).
+// forward stage leaves them untouched. F and FB hold per-element monomial
+// coefficients of the fields (to_monomial_kernel): the field and its
+// gradient at x are then one pass over the monomials. NODAL: also scatter
+// dL/dfield onto the nodes (per-warp shared staging of the Lagrange values
+// and gE/gB, summed over runs of lanes in one element, then one atomic per
+// run and node).
 template <int ORDER, bool NODAL>
-__global__ void __launch_bounds__(ADJ_BLOCK)
+__global__ void __launch_bounds__(ADJ_BLOCK, ORDER >= 4 ? 3 : ADJ_MIN_BLOCKS)
     lsrk_stage_adjoint_kernel(DevMesh M, const Lagrange<ORDER> L, Fields6 F, FieldBasis FB,
                               GradFields GF, long long n, const double *__restrict__ x,
                               const double *__restrict__ p, const uint32_t *__restrict__ el,
@@ -140,7 +170,7 @@ __global__ void __launch_bounds__(ADJ_BLOCK)
         gB[d] = dt * charge * t[d];
       }
     }
-    // monomials and their powers at the reference coordinates
+    // powers of the reference coordinates
     const double *A = M.inv_maps + 12 * (size_t)e;
     double r0, r1, r2;
     apply_map_exact(A, x[i], x[n + i], x[2 * n + i], r0, r1, r2);
@@ -152,62 +182,11 @@ __global__ void __launch_bounds__(ADJ_BLOCK)
       pw1[k] = pw1[k - 1] * r1;
       pw2[k] = pw2[k - 1] * r2;
     }
+    // one pass over the monomials (the fields come as per-element monomial
+    // coefficients): B(x), grad of h = gE . E + gB . B, basis projections
     double mono[NP];
-    {
-      int idx = 0;
-#pragma unroll
-      for (int cc = 0; cc <= ORDER; ++cc)
-#pragma unroll
-        for (int bb = 0; bb <= ORDER - cc; ++bb)
-#pragma unroll
-          for (int aa = 0; aa <= ORDER - bb - cc; ++aa) mono[idx++] = pw0[aa] * pw1[bb] * pw2[cc];
-    }
-    // node loop: Lagrange values, B(x), monomial coefficients of
-    // h = gE . E + gB . B, basis projections
-    double hh[NP];
-#pragma unroll
-    for (int j = 0; j < NP; ++j) hh[j] = 0;
-    double Bx[3] = {0, 0, 0};
+    double Bx[3] = {0, 0, 0}, gr[3] = {0, 0, 0};
     const size_t nb = (size_t)e * NP;
-#pragma unroll
-    for (int nd = 0; nd < NP; ++nd) {
-      double ln = 0;
-#pragma unroll
-      for (int j = 0; j < NP; ++j) ln = fma(L.w[nd * NP + j], mono[j], ln);
-      double fv[6];
-#pragma unroll
-      for (int k = 0; k < 6; ++k) fv[k] = F.f[k] ? __ldg(F.f[k] + nb + nd) : 0.0;
-      double h = 0;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        Bx[d] = fma(ln, fv[3 + d], Bx[d]);
-        h = fma(gE[d], fv[d], h);
-        h = fma(gB[d], fv[3 + d], h);
-      }
-#pragma unroll
-      for (int j = 0; j < NP; ++j) hh[j] = fma(h, L.w[nd * NP + j], hh[j]);
-#pragma unroll
-      for (int k = 0; k < PRT_MAX_FIELD_BASIS; ++k) {
-        if (k >= FB.count) break;
-        double hb = 0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          if (FB.f[k][d]) hb = fma(gE[d], __ldg(FB.f[k][d] + nb + nd), hb);
-          if (FB.f[k][3 + d]) hb = fma(gB[d], __ldg(FB.f[k][3 + d] + nb + nd), hb);
-        }
-        tb[k] = fma(ln, hb, tb[k]);
-      }
-      if (NODAL) wl[nd * 32 + lane] = ln;
-    }
-    if (NODAL) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        wg[d * 32 + lane] = gE[d];
-        wg[(3 + d) * 32 + lane] = gB[d];
-      }
-    }
-    // gradient of h in reference coordinates, then through the affine map
-    double gr[3] = {0, 0, 0};
     {
       int idx = 0;
 #pragma unroll
@@ -216,11 +195,48 @@ __global__ void __launch_bounds__(ADJ_BLOCK)
         for (int bb = 0; bb <= ORDER - cc; ++bb)
 #pragma unroll
           for (int aa = 0; aa <= ORDER - bb - cc; ++aa) {
-            const double hj = hh[idx++];
-            if (aa > 0) gr[0] = fma(hj, aa * pw0[aa - 1] * pw1[bb] * pw2[cc], gr[0]);
-            if (bb > 0) gr[1] = fma(hj, bb * pw0[aa] * pw1[bb - 1] * pw2[cc], gr[1]);
-            if (cc > 0) gr[2] = fma(hj, cc * pw0[aa] * pw1[bb] * pw2[cc - 1], gr[2]);
+            const double mj = pw0[aa] * pw1[bb] * pw2[cc];
+            if (NODAL) mono[idx] = mj;
+            double h = 0;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const double ce = F.f[d] ? __ldg(F.f[d] + nb + idx) : 0.0;
+              const double cb = F.f[3 + d] ? __ldg(F.f[3 + d] + nb + idx) : 0.0;
+              Bx[d] = fma(cb, mj, Bx[d]);
+              h = fma(gE[d], ce, h);
+              h = fma(gB[d], cb, h);
+            }
+            if (aa > 0) gr[0] = fma(h, aa * pw0[aa - 1] * pw1[bb] * pw2[cc], gr[0]);
+            if (bb > 0) gr[1] = fma(h, bb * pw0[aa] * pw1[bb - 1] * pw2[cc], gr[1]);
+            if (cc > 0) gr[2] = fma(h, cc * pw0[aa] * pw1[bb] * pw2[cc - 1], gr[2]);
+#pragma unroll
+            for (int k = 0; k < PRT_MAX_FIELD_BASIS; ++k) {
+              if (k >= FB.count) break;
+              double hb = 0;
+#pragma unroll
+              for (int d = 0; d < 3; ++d) {
+                if (FB.f[k][d]) hb = fma(gE[d], __ldg(FB.f[k][d] + nb + idx), hb);
+                if (FB.f[k][3 + d]) hb = fma(gB[d], __ldg(FB.f[k][3 + d] + nb + idx), hb);
+              }
+              tb[k] = fma(hb, mj, tb[k]);
+            }
+            ++idx;
           }
+    }
+    if (NODAL) {
+      // Lagrange values for the nodal scatter
+#pragma unroll
+      for (int nd = 0; nd < NP; ++nd) {
+        double ln = 0;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) ln = fma(L.w[nd * NP + j], mono[j], ln);
+        wl[nd * 32 + lane] = ln;
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        wg[d * 32 + lane] = gE[d];
+        wg[(3 + d) * 32 + lane] = gB[d];
+      }
     }
     double w[3];
     {
@@ -341,64 +357,159 @@ __global__ void contract_kernel(long long npos, long long nn,
   for (int d = 0; d < 4; ++d) G[d * npos + u] = s[d];
 }
 
-// Adjoint of the plain shape deposition, particle-centric (one warp per
-// particle): with weight w = q N and S = (a - r^2/a)^alpha,
+struct CentreBinsDev {
+  double origin[3], inv_w[3];
+  int dims[3];
+  double max_radius;
+  const uint32_t *__restrict__ starts;
+  const double *__restrict__ spheres;
+  const uint32_t *__restrict__ ranges;
+};
+
+constexpr int DEP_ADJ_BLOCK = 128;
+
+// Adjoint of the plain shape deposition. With weight w = q N and
+// S = (a - r^2/a)^alpha:
 //   dL/dx_p = w sum_u (G0_u + G_u . v_p) dS/dx_p,
 //   dL/dv_p = w sum_u G_u S,   dS/dx_p = alpha (a - r^2/a)^(alpha-1) (2/a) (x_u - x_p).
+// Lane = particle; a warp takes 32 consecutive particles (element-sorted
+// particles are spatially close) and walks the position groups whose centre
+// bin lies within a + (largest group radius) of the warp's bounding box: the
+// lanes test 32 candidate groups at a time against the box (ballot), then
+// for each surviving group that reaches some lane's particle the warp stages
+// the group's positions and node adjoints in shared memory and every lane
+// evaluates its particle against all of them, branch-free (zero weight
+// beyond the radius). Each particle's sums run in a fixed order: no atomics,
+// deterministic. Periodic axes: the warp also walks the images of its box
+// shifted by a period where the box comes within the radius of the
+// periodicity interval's end.
 template <bool ALPHA2>
-__global__ void deposit_adjoint_kernel(DevMesh M, prt_dep::TileBinsDev TB,
-                                       const double *__restrict__ pos, long long npos,
-                                       const double *__restrict__ boxes, prt_dep::ShapeParams S,
-                                       double normalizer, const double *__restrict__ G,
-                                       long long n, const double *__restrict__ x,
-                                       const double *__restrict__ q,
-                                       const double *__restrict__ v,
-                                       const uint32_t *__restrict__ el, double *__restrict__ lx,
-                                       double *__restrict__ lv) {
-  const long long i = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= n) return;  // whole warps leave together
-  if (el && el[i] == PRT_INVALID) return;
-  const double px = x[i], py = x[n + i], pz = x[2 * n + i];
-  const double v0 = v ? v[i] : 0, v1 = v ? v[n + i] : 0, v2 = v ? v[2 * n + i] : 0;
-  double ax0 = 0, ax1 = 0, ax2 = 0, as0 = 0, as1 = 0, as2 = 0, as3 = 0;
-  const double two_over_a = 2.0 * S.inv_radius;
-  prt_dep::visit_positions_in_reach(
-      M, TB, pos, npos, boxes, S, px, py, pz, lane,
-      [&](long long uu, double e0, double e1, double e2, double r2) {
-        const double rt = S.radius - r2 * S.inv_radius;
-        double sv, ds;
-        if (ALPHA2) {
-          sv = rt * rt;
-          ds = 2.0 * rt * two_over_a;
-        } else {
-          const double pm = pow(rt, S.alpha - 1.0);
-          sv = pm * rt;
-          ds = S.alpha * pm * two_over_a;
-        }
-        const double g0 = G[uu], g1 = G[npos + uu], g2 = G[2 * npos + uu],
-                     g3 = G[3 * npos + uu];
-        const double h = g0 + g1 * v0 + g2 * v1 + g3 * v2;
-        const double hd = h * ds;
-        ax0 = fma(hd, e0, ax0);
-        ax1 = fma(hd, e1, ax1);
-        ax2 = fma(hd, e2, ax2);
-        as0 = fma(g0, sv, as0);
-        as1 = fma(g1, sv, as1);
-        as2 = fma(g2, sv, as2);
-        as3 = fma(g3, sv, as3);
-      });
+__global__ void __launch_bounds__(DEP_ADJ_BLOCK, 4)
+    deposit_adjoint_kernel(DevMesh M, CentreBinsDev CB, const double *__restrict__ pos,
+                           long long npos, prt_dep::ShapeParams S, double normalizer,
+                           const double *__restrict__ G, long long n,
+                           const double *__restrict__ x, const double *__restrict__ q,
+                           const double *__restrict__ v, const uint32_t *__restrict__ el,
+                           double *__restrict__ lx, double *__restrict__ lv) {
+  __shared__ double2 stage[DEP_ADJ_BLOCK / 32][32][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long i = blockIdx.x * (long long)DEP_ADJ_BLOCK + threadIdx.x;
+  const bool live = i < n && (!el || el[i] != PRT_INVALID);
+  double p[3] = {0, 0, 0}, vv[3] = {0, 0, 0};
+  if (live) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    ax0 += __shfl_xor_sync(0xffffffffu, ax0, o);
-    ax1 += __shfl_xor_sync(0xffffffffu, ax1, o);
-    ax2 += __shfl_xor_sync(0xffffffffu, ax2, o);
-    as1 += __shfl_xor_sync(0xffffffffu, as1, o);
-    as2 += __shfl_xor_sync(0xffffffffu, as2, o);
-    as3 += __shfl_xor_sync(0xffffffffu, as3, o);
+    for (int d = 0; d < 3; ++d) {
+      p[d] = x[d * n + i];
+      if (v) vv[d] = v[d * n + i];
+    }
   }
-  (void)as0;
-  if (lane == 0) {
+  if (!__any_sync(0xffffffffu, live)) return;  // warp-uniform
+  double blo[3], bhi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    blo[d] = live ? p[d] : INFINITY;
+    bhi[d] = live ? p[d] : -INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      blo[d] = fmin(blo[d], __shfl_xor_sync(0xffffffffu, blo[d], o));
+      bhi[d] = fmax(bhi[d], __shfl_xor_sync(0xffffffffu, bhi[d], o));
+    }
+  }
+  int lo_img[3], hi_img[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    lo_img[d] = hi_img[d] = 0;
+    if (M.pmin[d] != M.pmax[d]) {
+      if (blo[d] - S.radius < M.pmin[d]) hi_img[d] = 1;
+      if (bhi[d] + S.radius > M.pmax[d]) lo_img[d] = -1;
+    }
+  }
+  const double reach = S.radius + CB.max_radius;
+  double ax0 = 0, ax1 = 0, ax2 = 0, as1 = 0, as2 = 0, as3 = 0;
+  for (int iz = lo_img[2]; iz <= hi_img[2]; ++iz)
+    for (int iy = lo_img[1]; iy <= hi_img[1]; ++iy)
+      for (int ix = lo_img[0]; ix <= hi_img[0]; ++ix) {
+        const double sh[3] = {ix * (M.pmax[0] - M.pmin[0]), iy * (M.pmax[1] - M.pmin[1]),
+                              iz * (M.pmax[2] - M.pmin[2])};
+        const double c0 = p[0] + sh[0], c1 = p[1] + sh[1], c2 = p[2] + sh[2];
+        double qlo[3], qhi[3];
+        int b0[3], b1[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          qlo[d] = blo[d] + sh[d];
+          qhi[d] = bhi[d] + sh[d];
+          const double l = floor((qlo[d] - reach - CB.origin[d]) * CB.inv_w[d]);
+          const double h = floor((qhi[d] + reach - CB.origin[d]) * CB.inv_w[d]);
+          b0[d] = (int)fmax(0.0, fmin(l, CB.dims[d] - 1.0));
+          b1[d] = (int)fmax(0.0, fmin(h, CB.dims[d] - 1.0));
+        }
+        for (int bz = b0[2]; bz <= b1[2]; ++bz)
+          for (int by = b0[1]; by <= b1[1]; ++by) {
+            const long long row = (long long)CB.dims[0] * (by + (long long)CB.dims[1] * bz);
+            const uint32_t k0 = CB.starts[row + b0[0]], k1 = CB.starts[row + b1[0] + 1];
+            for (uint32_t kb = k0; kb < k1; kb += 32) {
+              const uint32_t k = kb + lane;
+              bool cand = false;
+              if (k < k1) {
+                const double *sp = CB.spheres + 4 * (size_t)k;
+                double d2 = 0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                  const double e = fmax(0.0, fmax(qlo[d] - sp[d], sp[d] - qhi[d]));
+                  d2 = fma(e, e, d2);
+                }
+                const double lim = S.radius + sp[3];
+                cand = d2 <= lim * lim;
+              }
+              unsigned mask = __ballot_sync(0xffffffffu, cand);
+              while (mask) {
+                const int j = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const uint32_t kk = kb + j;
+                const double *sp = CB.spheres + 4 * (size_t)kk;
+                const double e0 = sp[0] - c0, e1 = sp[1] - c1, e2 = sp[2] - c2;
+                const double lim = S.radius + sp[3];
+                const bool hit = live && e0 * e0 + e1 * e1 + e2 * e2 <= lim * lim;
+                if (!__any_sync(0xffffffffu, hit)) continue;
+                const uint32_t u0 = CB.ranges[2 * (size_t)kk], cnt = CB.ranges[2 * (size_t)kk + 1];
+                if ((uint32_t)lane < cnt) {
+                  const long long u = u0 + lane;
+                  stage[warp][lane][0] = make_double2(pos[3 * u], pos[3 * u + 1]);
+                  stage[warp][lane][1] = make_double2(pos[3 * u + 2], G[u]);
+                  stage[warp][lane][2] = make_double2(G[npos + u], G[2 * npos + u]);
+                  stage[warp][lane][3] = make_double2(G[3 * npos + u], 0.0);
+                }
+                __syncwarp();
+                for (uint32_t t = 0; t < cnt; ++t) {
+                  const double2 s0 = stage[warp][t][0], s1 = stage[warp][t][1],
+                                s2 = stage[warp][t][2], s3 = stage[warp][t][3];
+                  const double f0 = s0.x - c0, f1 = s0.y - c1, f2 = s1.x - c2;
+                  const double r2 = fma(f0, f0, fma(f1, f1, f2 * f2));
+                  const double rt = fmax(fma(-r2, S.inv_radius, S.radius), 0.0);
+                  double sv, ds;
+                  if (ALPHA2) {
+                    sv = rt * rt;
+                    ds = rt * (4.0 * S.inv_radius);
+                  } else {
+                    const double pm = rt > 0 ? pow(rt, S.alpha - 1.0) : 0.0;
+                    sv = pm * rt;
+                    ds = S.alpha * pm * (2.0 * S.inv_radius);
+                  }
+                  const double h = fma(s2.y, vv[1], fma(s2.x, vv[0], fma(s3.x, vv[2], s1.y)));
+                  const double hd = h * ds;
+                  ax0 = fma(hd, f0, ax0);
+                  ax1 = fma(hd, f1, ax1);
+                  ax2 = fma(hd, f2, ax2);
+                  as1 = fma(s2.x, sv, as1);
+                  as2 = fma(s2.y, sv, as2);
+                  as3 = fma(s3.x, sv, as3);
+                }
+                __syncwarp();
+              }
+            }
+          }
+      }
+  if (live) {
     const double w = q[i] * normalizer;
     lx[i] += w * ax0;
     lx[n + i] += w * ax1;
@@ -500,18 +611,19 @@ extern "C" int prt_lsrk_stage_adjoint(const prt_pusher *P, prt_workspace *ws, in
                                       const double *x, const double *p, const uint32_t *el,
                                       const double *q, const double *m, double *lam_x,
                                       double *lam_p, double *lam_kx, double *lam_kp,
-                                      const double *const fields[6], double a, double b,
-                                      double dt, double c, double *const grad_fields[6],
-                                      int32_t nbasis, const double *const *basis,
-                                      double *grad_theta, void *stream) {
-  if (!P || !ws || n < 0 || !fields) return PRT_ERR_INVALID_ARGUMENT;
+                                      const double *const field_coefficients[6], double a,
+                                      double b, double dt, double c,
+                                      double *const grad_fields[6], int32_t nbasis,
+                                      const double *const *basis, double *grad_theta,
+                                      void *stream) {
+  if (!P || !ws || n < 0 || !field_coefficients) return PRT_ERR_INVALID_ARGUMENT;
   if (nbasis < 0 || nbasis > PRT_MAX_FIELD_BASIS || (nbasis > 0 && (!basis || !grad_theta)))
     return PRT_ERR_INVALID_ARGUMENT;
   if (n == 0) return PRT_OK;
   if (!x || !p || !el || !q || !m || !lam_x || !lam_p || !lam_kx || !lam_kp)
     return PRT_ERR_INVALID_ARGUMENT;
   Fields6 F;
-  for (int k = 0; k < 6; ++k) F.f[k] = fields[k];
+  for (int k = 0; k < 6; ++k) F.f[k] = field_coefficients[k];
   FieldBasis FB;
   FB.count = nbasis;
   for (int k = 0; k < PRT_MAX_FIELD_BASIS; ++k)
@@ -528,6 +640,35 @@ extern "C" int prt_lsrk_stage_adjoint(const prt_pusher *P, prt_workspace *ws, in
     case 2: return dispatch_adjoint<2>(nodal, P, ws, n, x, p, el, q, m, lam_x, lam_p, lam_kx, lam_kp, F, FB, GF, a, b, dt, c, grad_theta, s);
     case 3: return dispatch_adjoint<3>(nodal, P, ws, n, x, p, el, q, m, lam_x, lam_p, lam_kx, lam_kp, F, FB, GF, a, b, dt, c, grad_theta, s);
     case 4: return dispatch_adjoint<4>(nodal, P, ws, n, x, p, el, q, m, lam_x, lam_p, lam_kx, lam_kp, F, FB, GF, a, b, dt, c, grad_theta, s);
+  }
+  return PRT_ERR_INVALID_ARGUMENT;
+}
+
+template <int ORDER>
+static int launch_to_monomial(const prt_pusher *P, int32_t count, const double *const *fields,
+                              double *const *coefficients, cudaStream_t s) {
+  const long long E = P->mesh->dev.E;
+  const Lagrange<ORDER> L = make_lagrange<ORDER>(P);
+  for (int k = 0; k < count; ++k) {
+    if (!fields[k] || !coefficients[k]) continue;
+    to_monomial_kernel<ORDER><<<prt_grid_blocks(E, 128), 128, 0, s>>>(L, E, fields[k],
+                                                                    coefficients[k]);
+    PRT_CHECK_CUDA(cudaGetLastError());
+  }
+  return PRT_OK;
+}
+
+extern "C" int prt_fields_to_monomial(const prt_pusher *P, int32_t count,
+                                      const double *const *fields, double *const *coefficients,
+                                      void *stream) {
+  if (!P || count < 0 || (count > 0 && (!fields || !coefficients)))
+    return PRT_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  switch (P->order) {
+    case 1: return launch_to_monomial<1>(P, count, fields, coefficients, s);
+    case 2: return launch_to_monomial<2>(P, count, fields, coefficients, s);
+    case 3: return launch_to_monomial<3>(P, count, fields, coefficients, s);
+    case 4: return launch_to_monomial<4>(P, count, fields, coefficients, s);
   }
   return PRT_ERR_INVALID_ARGUMENT;
 }
@@ -568,25 +709,26 @@ extern "C" int prt_deposit_shape_adjoint(const prt_mesh *mesh, prt_workspace *ws
   S.inv_radius = 1.0 / shape.radius;
   S.alpha = shape.alpha;
   for (int d = 0; d < 3; ++d) S.reach[d] = shape.radius;
-  prt_dep::TileBinsDev TB;
+  const auto &H = PS.centre_bins;
+  CentreBinsDev CB;
   for (int d = 0; d < 3; ++d) {
-    TB.origin[d] = PS.bins.origin[d];
-    TB.inv_w[d] = PS.bins.inv_w[d];
-    TB.dims[d] = PS.bins.dims[d];
+    CB.origin[d] = H.origin[d];
+    CB.inv_w[d] = H.inv_w[d];
+    CB.dims[d] = H.dims[d];
   }
-  TB.starts = PS.bins.starts;
-  TB.tiles = PS.bins.tiles;
+  CB.max_radius = H.max_radius;
+  CB.starts = H.starts;
+  CB.spheres = H.spheres;
+  CB.ranges = H.ranges;
   const double *vv = grad_j ? v : nullptr;
   double *lvv = grad_j ? lam_v : nullptr;
-  const long long threads = 32 * (long long)n;
+  const unsigned blocks = (unsigned)((n + DEP_ADJ_BLOCK - 1) / DEP_ADJ_BLOCK);
   if (shape.alpha == 2)
-    deposit_adjoint_kernel<true><<<prt_grid_blocks(threads, 128), 128, 0, s>>>(
-        mesh->dev, TB, PS.pos, PS.count, PS.tile_boxes, S, shape.normalizer, G, n, x, q, vv, el,
-        lam_x, lvv);
+    deposit_adjoint_kernel<true><<<blocks, DEP_ADJ_BLOCK, 0, s>>>(
+        mesh->dev, CB, PS.pos, PS.count, S, shape.normalizer, G, n, x, q, vv, el, lam_x, lvv);
   else
-    deposit_adjoint_kernel<false><<<prt_grid_blocks(threads, 128), 128, 0, s>>>(
-        mesh->dev, TB, PS.pos, PS.count, PS.tile_boxes, S, shape.normalizer, G, n, x, q, vv, el,
-        lam_x, lvv);
+    deposit_adjoint_kernel<false><<<blocks, DEP_ADJ_BLOCK, 0, s>>>(
+        mesh->dev, CB, PS.pos, PS.count, S, shape.normalizer, G, n, x, q, vv, el, lam_x, lvv);
   PRT_CHECK_CUDA(cudaGetLastError());
   return PRT_OK;
 }

@@ -142,7 +142,8 @@ extern "C" int prt_mesh_destroy(prt_mesh *m) {
                         m->dev.vadj, m->dev.nodes, m->dev.bin_starts,
                         m->dev.bin_elements, m->face_centroids, m->face_radii,
                         P.pos, P.node_to_pos, P.run_starts, P.run_nodes, P.tile_boxes,
-                        P.group_starts, P.group_spheres, P.bins.starts, P.bins.tiles};
+                        P.group_starts, P.group_spheres, P.bins.starts, P.bins.tiles,
+                        P.centre_bins.starts, P.centre_bins.spheres, P.centre_bins.ranges};
   for (const void *p : ptrs)
     if (p) cudaFree((void *)p);
   delete m;
@@ -181,6 +182,10 @@ static void fold_timer(KernelTimer &T) {
 
 ScopedTimer::ScopedTimer(prt_workspace *w, int c, cudaStream_t st) : ws(w), cat(c), s(st) {
   if (!ws || !ws->timing || c < 0 || c >= PRT_TIME_CATEGORIES) return;
+  // launches captured into a CUDA graph are not timed (the ring's
+  // synchronising fold is not allowed while capturing)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return;
   KernelTimer &T = ws->timers[c];
   if (!T.created) {
     for (int i = 0; i < KernelTimer::RING; ++i) {

@@ -862,6 +862,50 @@ int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
     P.groups = groups;
     if ((rc = upload_vec(gstart, &P.group_starts))) return rc;
     if ((rc = upload_vec(spheres, &P.group_spheres))) return rc;
+
+    // centre bins: width about the mean group radius
+    auto &CB = P.centre_bins;
+    double rsum = 0, rmax = 0;
+    for (long long g = 0; g < groups; ++g) {
+      rsum += spheres[4 * g + 3];
+      rmax = std::max(rmax, spheres[4 * g + 3]);
+    }
+    const double wbin = std::max(rsum / std::max<long long>(1, groups), 1e-300);
+    long long ncb = 1;
+    for (int a = 0; a < 3; ++a) {
+      const double e = m->box_hi[a] - m->box_lo[a];
+      const int dims = e > 0 ? (int)std::max(1.0, std::min(1024.0, std::floor(e / wbin))) : 1;
+      CB.dims[a] = dims;
+      CB.origin[a] = m->box_lo[a];
+      CB.inv_w[a] = e > 0 ? dims / e : 0.0;
+      ncb *= dims;
+    }
+    CB.max_radius = rmax;
+    std::vector<uint32_t> gbin(std::max<long long>(1, groups));
+    std::vector<uint32_t> cstarts(ncb + 1, 0);
+    for (long long g = 0; g < groups; ++g) {
+      long long b = 0, mul = 1;
+      for (int a = 0; a < 3; ++a) {
+        const double u = std::floor((spheres[4 * g + a] - CB.origin[a]) * CB.inv_w[a]);
+        b += mul * (long long)std::max(0.0, std::min(u, CB.dims[a] - 1.0));
+        mul *= CB.dims[a];
+      }
+      gbin[g] = (uint32_t)b;
+      ++cstarts[b + 1];
+    }
+    for (long long b = 0; b < ncb; ++b) cstarts[b + 1] += cstarts[b];
+    std::vector<uint32_t> fill(cstarts.begin(), cstarts.end() - 1);
+    std::vector<double> csph(4 * (size_t)std::max<long long>(1, groups));
+    std::vector<uint32_t> crange(2 * (size_t)std::max<long long>(1, groups));
+    for (long long g = 0; g < groups; ++g) {
+      const uint32_t k = fill[gbin[g]]++;
+      for (int a = 0; a < 4; ++a) csph[4 * k + a] = spheres[4 * g + a];
+      crange[2 * k] = gstart[g];
+      crange[2 * k + 1] = gstart[g + 1] - gstart[g];
+    }
+    if ((rc = upload_vec(cstarts, &CB.starts))) return rc;
+    if ((rc = upload_vec(csph, &CB.spheres))) return rc;
+    if ((rc = upload_vec(crange, &CB.ranges))) return rc;
   }
 
   // uniform bins of about one tile listing the tiles whose box meets them

@@ -49,6 +49,17 @@ struct PositionSet {
   long long groups = 0;
   const uint32_t *group_starts = nullptr; // [groups + 1]
   const double *group_spheres = nullptr;  // [groups][4]: centre xyz, radius
+  // the groups binned by the bin of their sphere centre (each group in
+  // exactly one bin; uniform bins of about a group radius), in bin order:
+  // spheres and position ranges, with CSR bin starts
+  struct {
+    double origin[3], inv_w[3];
+    int dims[3];
+    double max_radius = 0;
+    const uint32_t *starts = nullptr;   // [nbins + 1]
+    const double *spheres = nullptr;    // [groups][4], bin order
+    const uint32_t *ranges = nullptr;   // [groups][2]: first position, count
+  } centre_bins;
 };
 
 struct prt_mesh {
