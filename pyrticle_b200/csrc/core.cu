@@ -143,7 +143,8 @@ extern "C" int prt_mesh_destroy(prt_mesh *m) {
                         m->dev.bin_elements, m->face_centroids, m->face_radii,
                         P.pos, P.node_to_pos, P.run_starts, P.run_nodes, P.tile_boxes,
                         P.group_starts, P.group_spheres, P.bins.starts, P.bins.tiles,
-                        P.centre_bins.starts, P.centre_bins.spheres, P.centre_bins.ranges};
+                        P.centre_bins.starts, P.centre_bins.spheres, P.centre_bins.ranges,
+                        P.wide_starts, P.wide_spheres};
   for (const void *p : ptrs)
     if (p) cudaFree((void *)p);
   delete m;

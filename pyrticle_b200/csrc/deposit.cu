@@ -179,8 +179,150 @@ constexpr int WARPS = BLOCK / 32;
 #ifndef PRT_GATHER_MIN_BLOCKS
 #define PRT_GATHER_MIN_BLOCKS 6
 #endif
+// the same for the two-positions-per-lane form (twice the accumulators)
+#ifndef PRT_GATHER_MIN_BLOCKS_WIDE
+#define PRT_GATHER_MIN_BLOCKS_WIDE 4
+#endif
+#ifndef PRT_MIXED_MIN_BLOCKS_WIDE
+#define PRT_MIXED_MIN_BLOCKS_WIDE 8
+#endif
+// positions per lane of the FP64 and mixed deposition (2: wide groups)
+#ifndef PRT_FP64_PPL
+#define PRT_FP64_PPL 2
+#endif
+#ifndef PRT_MIXED_PPL
+#define PRT_MIXED_PPL 2
+#endif
+// unrolling of the full-batch loops (two entries per step)
+#ifndef PRT_FP64_UNROLL
+#define PRT_FP64_UNROLL 4
+#endif
+#ifndef PRT_MIXED_UNROLL
+#define PRT_MIXED_UNROLL 2
+#endif
+constexpr int FP64_UNROLL = PRT_FP64_UNROLL;
+constexpr int MIXED_UNROLL = PRT_MIXED_UNROLL;
 // per-warp ring of compacted particles (two batches of 32)
 constexpr int RING = 64;
+
+// Streams the candidate particles of one warp's position group: the
+// particles of the bin rows that can come within `radius` of the group's box
+// [c + lo, c + hi], 32 at a time (one per lane, straight from L2/L1). Calls
+// visit(in, k, w0, w1, w2, d2) on every lane for every batch (warp-uniform),
+// with w the particle's position relative to c (periodic images shifted by
+// the period), d2 = |w|^2 and `in` set when the particle lies within the
+// radius of the box, hence possibly within the radius of a position.
+template <class Visit>
+__device__ __forceinline__ void stream_box(const BinGrid &G, const DepParticles &P,
+                                           const double c[3], const double lo[3],
+                                           const double hi[3], double radius, int lane,
+                                           Visit &&visit) {
+  const double rc = radius * (1 + 1e-9), rc2 = rc * rc;
+  const double rr = radius * (1 + 1e-6), rr2 = rr * rr;
+  int ulo[3], uhi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    ulo[d] = bin_floor(G, d, c[d] + lo[d] - radius);
+    uhi[d] = bin_floor(G, d, c[d] + hi[d] + radius);
+    if (G.periodic[d]) {
+      ulo[d] -= 1;
+      uhi[d] += 1;
+    } else {
+      ulo[d] = max(ulo[d], 0);
+      uhi[d] = min(uhi[d], G.dims[d] - 1);
+    }
+  }
+  const double2 *__restrict__ pay = reinterpret_cast<const double2 *>(P.payload);
+  // distance from the slab [blo, blo + w) of bins to the box along one axis
+  auto slab_gap = [&](int d, double blo) {
+    const double e = fmax(0.0, fmax(blo - (c[d] + hi[d]), (c[d] + lo[d]) - (blo + G.w[d]))) -
+                     G.slack[d];
+    return e > 0 ? e * e : 0.0;
+  };
+  for (int bz = ulo[2]; bz <= uhi[2]; ++bz) {
+    int wz = bz, qz = 0;
+    if (G.periodic[2]) { qz = floor_div(bz, G.dims[2]); wz = bz - qz * G.dims[2]; }
+    const double sz = qz * G.period[2] - c[2];
+    const double dz2 = slab_gap(2, G.origin[2] + bz * G.w[2]);
+    if (dz2 > rr2) continue;
+    for (int by = ulo[1]; by <= uhi[1]; ++by) {
+      int wy = by, qy = 0;
+      if (G.periodic[1]) { qy = floor_div(by, G.dims[1]); wy = by - qy * G.dims[1]; }
+      const double sy = qy * G.period[1] - c[1];
+      const double dyz2 = dz2 + slab_gap(1, G.origin[1] + by * G.w[1]);
+      if (dyz2 > rr2) continue;
+      const double rem = sqrt(rr2 - dyz2);
+      int bx0 = bin_floor(G, 0, c[0] + lo[0] - rem);
+      int bx1 = bin_floor(G, 0, c[0] + hi[0] + rem);
+      if (G.periodic[0]) {
+        bx0 -= 1;
+        bx1 += 1;
+      }
+      bx0 = max(bx0, ulo[0]);
+      bx1 = min(bx1, uhi[0]);
+      int bx = bx0;
+      while (bx <= bx1) {
+        int wx = bx, qx = 0, seg_end = bx1;
+        if (G.periodic[0]) {
+          qx = floor_div(bx, G.dims[0]);
+          wx = bx - qx * G.dims[0];
+          seg_end = min(bx1, (qx + 1) * G.dims[0] - 1);
+        }
+        const double sx = qx * G.period[0] - c[0];
+        const long long row = (long long)G.dims[0] * (wy + (long long)G.dims[1] * wz);
+        const uint32_t s0 = P.starts[row + wx];
+        const uint32_t s1 = P.starts[row + wx + (seg_end - bx) + 1];
+        bx = seg_end + 1;
+        for (uint32_t b0 = s0; b0 < s1; b0 += 32) {
+          const uint32_t k = b0 + lane;
+          bool in = false;
+          double w0 = 0, w1 = 0, w2 = 0, d2 = 0;
+          if (k < s1) {
+            const double2 xy = pay[4 * (size_t)k], zq = pay[4 * (size_t)k + 1];
+            w0 = xy.x + sx;
+            w1 = xy.y + sy;
+            w2 = zq.x + sz;
+            d2 = w0 * w0 + w1 * w1 + w2 * w2;
+            const double e0 = fmax(0.0, fmax(lo[0] - w0, w0 - hi[0]));
+            const double e1 = fmax(0.0, fmax(lo[1] - w1, w1 - hi[1]));
+            const double e2 = fmax(0.0, fmax(lo[2] - w2, w2 - hi[2]));
+            in = e0 * e0 + e1 * e1 + e2 * e2 <= rc2;
+          }
+          visit(in, k, w0, w1, w2, d2);
+        }
+      }
+    }
+  }
+}
+
+// Bounding box [lo, hi] (relative to c) of the positions a warp holds.
+template <int PPL>
+__device__ __forceinline__ void warp_box(const double *__restrict__ pos, uint32_t p0, int npg,
+                                         int lane, const double c[3], double lo[3],
+                                         double hi[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = INFINITY;
+    hi[d] = -INFINITY;
+  }
+#pragma unroll
+  for (int h = 0; h < PPL; ++h)
+    if (lane + 32 * h < npg) {
+      const long long u = p0 + lane + 32 * h;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = fmin(lo[d], pos[3 * u + d] - c[d]);
+        hi[d] = fmax(hi[d], pos[3 * u + d] - c[d]);
+      }
+    }
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+}
 
 // One warp per position group (<= 32 positions, one per lane), warps fully
 // independent (no block-level barrier). The warp streams the particles of
@@ -194,8 +336,8 @@ constexpr int RING = 64;
 // In COUNT mode counters[0] receives the (particle, position) pairs within
 // the radius, counters[1] the (particle, node) pairs (positions weighted by
 // their node count) and counters[2] the evaluated pairs.
-template <bool ALPHA2, bool COUNT>
-__global__ void __launch_bounds__(BLOCK, PRT_GATHER_MIN_BLOCKS)
+template <bool ALPHA2, bool COUNT, int PPL = 1>
+__global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_GATHER_MIN_BLOCKS_WIDE)
     deposit_groups_kernel(const double *__restrict__ pos, long long ngroups,
                           const uint32_t *__restrict__ gstarts,
                           const double *__restrict__ gspheres,
@@ -210,176 +352,111 @@ __global__ void __launch_bounds__(BLOCK, PRT_GATHER_MIN_BLOCKS)
   if (g >= ngroups) return;  // whole warp
   const uint32_t p0 = gstarts[g];
   const int npg = (int)(gstarts[g + 1] - p0);
-  const bool live = lane < npg;
   double2(*R)[RING] = ring[wid];
 
   const double c0 = gspheres[4 * g], c1 = gspheres[4 * g + 1], c2 = gspheres[4 * g + 2];
-  const double reach = S.radius + gspheres[4 * g + 3];
-  const double cull2 = (reach * (1 + 1e-9)) * (reach * (1 + 1e-9));
-  double U0 = 0, U1 = 0, U2 = 0, A = 0;
-  unsigned mult = 0;
-  if (live) {
-    const long long u = p0 + lane;
-    const double u0 = pos[3 * u] - c0, u1 = pos[3 * u + 1] - c1, u2 = pos[3 * u + 2] - c2;
-    A = u0 * u0 + u1 * u1 + u2 * u2;
-    U0 = -2 * u0;
-    U1 = -2 * u1;
-    U2 = -2 * u2;
-    if (COUNT) mult = run_starts[u + 1] - run_starts[u];
+  // lane holds positions p0 + lane + 32 h, h < PPL. With u = x_position - c
+  // and w = x_particle - c: a - r^2/a = (a - |u|^2/a) - |w|^2/a + (2/a) u.w,
+  // so per pair the weight base is three FMAs and an add: B + e + V . w
+  double V0[PPL], V1[PPL], V2[PPL], B[PPL];
+  bool live[PPL];
+  unsigned mult[PPL];
+#pragma unroll
+  for (int h = 0; h < PPL; ++h) {
+    live[h] = lane + 32 * h < npg;
+    V0[h] = V1[h] = V2[h] = B[h] = 0;
+    mult[h] = 0;
+    if (live[h]) {
+      const long long u = p0 + lane + 32 * h;
+      const double u0 = pos[3 * u] - c0, u1 = pos[3 * u + 1] - c1, u2 = pos[3 * u + 2] - c2;
+      B[h] = S.radius - (u0 * u0 + u1 * u1 + u2 * u2) * S.inv_radius;
+      V0[h] = 2 * u0 * S.inv_radius;
+      V1[h] = 2 * u1 * S.inv_radius;
+      V2[h] = 2 * u2 * S.inv_radius;
+      if (COUNT) mult[h] = run_starts[u + 1] - run_starts[u];
+    }
   }
 
-  double r0 = 0, x0 = 0, y0 = 0, z0 = 0, r1 = 0, x1 = 0, y1 = 0, z1 = 0;
+  double r0[PPL], x0[PPL], y0[PPL], z0[PPL], r1[PPL], x1[PPL], y1[PPL], z1[PPL];
+#pragma unroll
+  for (int h = 0; h < PPL; ++h) r0[h] = x0[h] = y0[h] = z0[h] = r1[h] = x1[h] = y1[h] = z1[h] = 0;
   unsigned long long npairs = 0, nnode = 0, nevals = 0;
-  const double neg_inv_a = -S.inv_radius, rad = S.radius, rad2 = S.radius2;
 
-  auto weight = [&](double r2) -> double {
-    const double tr = fma(r2, neg_inv_a, rad);
+  // shape weight from tr = a - r^2/a (zero beyond the radius)
+  auto weight = [&](double tr) -> double {
     if (ALPHA2) {
       const double tp = fmax(tr, 0.0);
       return tp * tp;
     }
     return tr > 0 ? pow(tr, S.alpha) : 0.0;
   };
+  // one ring entry against the lane's positions
+  auto pair = [&](const double2 p, const double2 q, const double2 wq, const double2 wv,
+                  double *r, double *x, double *y, double *z) {
+#pragma unroll
+    for (int h = 0; h < PPL; ++h) {
+      const double tr = fma(V0[h], p.x, fma(V1[h], p.y, fma(V2[h], q.x, B[h] + q.y)));
+      const double sw = weight(tr);
+      r[h] = fma(wq.x, sw, r[h]);
+      x[h] = fma(wq.y, sw, x[h]);
+      y[h] = fma(wv.x, sw, y[h]);
+      z[h] = fma(wv.y, sw, z[h]);
+      if (COUNT) {
+        const unsigned in = live[h] && tr >= 0;
+        npairs += in;
+        nnode += in * mult[h];
+      }
+    }
+  };
   int head = 0, count = 0;
   // walks `k` ring entries from head (warp-uniform k)
   auto drain = [&](int k) {
-    int i = 0;
-    for (; i + 1 < k; i += 2) {
-      const int ea = (head + i) & (RING - 1), eb = (head + i + 1) & (RING - 1);
-      const double2 pa = R[0][ea], qa = R[1][ea], pb = R[0][eb], qb = R[1][eb];
-      const double r2a = fma(U0, pa.x, fma(U1, pa.y, fma(U2, qa.x, A + qa.y)));
-      const double r2b = fma(U0, pb.x, fma(U1, pb.y, fma(U2, qb.x, A + qb.y)));
-      const double sa = weight(r2a), sb = weight(r2b);
-      const double2 wa = R[2][ea], va = R[3][ea], wb = R[2][eb], vb = R[3][eb];
-      r0 = fma(wa.x, sa, r0);
-      x0 = fma(wa.y, sa, x0);
-      y0 = fma(va.x, sa, y0);
-      z0 = fma(va.y, sa, z0);
-      r1 = fma(wb.x, sb, r1);
-      x1 = fma(wb.y, sb, x1);
-      y1 = fma(vb.x, sb, y1);
-      z1 = fma(vb.y, sb, z1);
-      if (COUNT) {
-        const unsigned ia = live && r2a <= rad2, ib = live && r2b <= rad2;
-        npairs += ia + ib;
-        nnode += (ia + ib) * mult;
-      }
-    }
-    if (i < k) {
-      const int ea = (head + i) & (RING - 1);
-      const double2 pa = R[0][ea], qa = R[1][ea];
-      const double r2a = fma(U0, pa.x, fma(U1, pa.y, fma(U2, qa.x, A + qa.y)));
-      const double sa = weight(r2a);
-      const double2 wa = R[2][ea], va = R[3][ea];
-      r0 = fma(wa.x, sa, r0);
-      x0 = fma(wa.y, sa, x0);
-      y0 = fma(va.x, sa, y0);
-      z0 = fma(va.y, sa, z0);
-      if (COUNT) {
-        const unsigned ia = live && r2a <= rad2;
-        npairs += ia;
-        nnode += ia * mult;
-      }
+    for (int i = 0; i < k; ++i) {
+      const int e = (head + i) & (RING - 1);
+      pair(R[0][e], R[1][e], R[2][e], R[3][e], r0, x0, y0, z0);
     }
     if (COUNT && lane == 0) nevals += (unsigned long long)k * (unsigned)npg;
     head = (head + k) & (RING - 1);
     count -= k;
   };
+  // a full batch of 32 from head (0 or 32): constant offsets, two entries
+  // per step into two sets of accumulators
+  auto drain_full = [&]() {
+    const double2 *E0 = &R[0][head], *E1 = &R[1][head], *E2 = &R[2][head], *E3 = &R[3][head];
+#pragma unroll FP64_UNROLL
+    for (int i = 0; i < 32; i += 2) {
+      pair(E0[i], E1[i], E2[i], E3[i], r0, x0, y0, z0);
+      pair(E0[i + 1], E1[i + 1], E2[i + 1], E3[i + 1], r1, x1, y1, z1);
+    }
+    if (COUNT && lane == 0) nevals += 32ull * (unsigned)npg;
+    head = (head + 32) & (RING - 1);
+    count -= 32;
+  };
 
   const double cc[3] = {c0, c1, c2};
-  int ulo[3], uhi[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    ulo[d] = bin_floor(G, d, cc[d] - reach);
-    uhi[d] = bin_floor(G, d, cc[d] + reach);
-    if (G.periodic[d]) {
-      ulo[d] -= 1;
-      uhi[d] += 1;
-    } else {
-      ulo[d] = max(ulo[d], 0);
-      uhi[d] = min(uhi[d], G.dims[d] - 1);
-    }
-  }
-  const double reach_c = reach * (1 + 1e-6);
-  const double reach_c2 = reach_c * reach_c;
+  double blo[3], bhi[3];
+  warp_box<PPL>(pos, p0, npg, lane, cc, blo, bhi);
   const double2 *__restrict__ pay = reinterpret_cast<const double2 *>(P.payload);
-
-  for (int bz = ulo[2]; bz <= uhi[2]; ++bz) {
-    int wz = bz, qz = 0;
-    if (G.periodic[2]) { qz = floor_div(bz, G.dims[2]); wz = bz - qz * G.dims[2]; }
-    const double sz = qz * G.period[2] - c2;
-    double dz2;
-    {
-      const double blo = G.origin[2] + bz * G.w[2], bhi = blo + G.w[2];
-      const double e = fmax(0.0, fmax(blo - c2, c2 - bhi)) - G.slack[2];
-      dz2 = e > 0 ? e * e : 0.0;
-      if (dz2 > reach_c2) continue;
-    }
-    for (int by = ulo[1]; by <= uhi[1]; ++by) {
-      int wy = by, qy = 0;
-      if (G.periodic[1]) { qy = floor_div(by, G.dims[1]); wy = by - qy * G.dims[1]; }
-      const double sy = qy * G.period[1] - c1;
-      int bx0, bx1;
-      {
-        const double blo = G.origin[1] + by * G.w[1], bhi = blo + G.w[1];
-        const double e = fmax(0.0, fmax(blo - c1, c1 - bhi)) - G.slack[1];
-        const double dyz2 = dz2 + (e > 0 ? e * e : 0.0);
-        if (dyz2 > reach_c2) continue;
-        const double rem = sqrt(reach_c2 - dyz2);
-        bx0 = bin_floor(G, 0, c0 - rem);
-        bx1 = bin_floor(G, 0, c0 + rem);
-        if (G.periodic[0]) {
-          bx0 -= 1;
-          bx1 += 1;
-        }
-        bx0 = max(bx0, ulo[0]);
-        bx1 = min(bx1, uhi[0]);
-      }
-      int bx = bx0;
-      while (bx <= bx1) {
-        int wx = bx, qx = 0, seg_end = bx1;
-        if (G.periodic[0]) {
-          qx = floor_div(bx, G.dims[0]);
-          wx = bx - qx * G.dims[0];
-          seg_end = min(bx1, (qx + 1) * G.dims[0] - 1);
-        }
-        const double sx = qx * G.period[0] - c0;
-        const long long row = (long long)G.dims[0] * (wy + (long long)G.dims[1] * wz);
-        const uint32_t s0 = P.starts[row + wx];
-        const uint32_t s1 = P.starts[row + wx + (seg_end - bx) + 1];
-        bx = seg_end + 1;
-        for (uint32_t b0 = s0; b0 < s1; b0 += 32) {
-          const uint32_t k = b0 + lane;
-          bool in = false;
-          double w0 = 0, w1 = 0, w2 = 0, d2 = 0, qn = 0;
-          if (k < s1) {
-            const double2 xy = pay[4 * (size_t)k], zq = pay[4 * (size_t)k + 1];
-            w0 = xy.x + sx;
-            w1 = xy.y + sy;
-            w2 = zq.x + sz;
-            qn = zq.y;
-            d2 = w0 * w0 + w1 * w1 + w2 * w2;
-            in = d2 <= cull2;
-          }
-          const unsigned bal = __ballot_sync(0xffffffffu, in);
-          if (in) {
-            const double2 jv = pay[4 * (size_t)k + 2], jt = pay[4 * (size_t)k + 3];
-            const int slot = (head + count + __popc(bal & ((1u << lane) - 1u))) & (RING - 1);
-            R[0][slot] = make_double2(w0, w1);
-            R[1][slot] = make_double2(w2, d2);
-            R[2][slot] = make_double2(qn, jv.x);
-            R[3][slot] = make_double2(jv.y, jt.x);
-          }
-          count += __popc(bal);
-          __syncwarp();
-          if (count >= 32) {
-            drain(32);
-            __syncwarp();
-          }
-        }
-      }
-    }
-  }
+  stream_box(G, P, cc, blo, bhi, S.radius, lane,
+             [&](bool in, uint32_t k, double w0, double w1, double w2, double d2) {
+               const unsigned bal = __ballot_sync(0xffffffffu, in);
+               if (in) {
+                 const double2 zq = pay[4 * (size_t)k + 1];
+                 const double2 jv = pay[4 * (size_t)k + 2], jt = pay[4 * (size_t)k + 3];
+                 const int slot =
+                     (head + count + __popc(bal & ((1u << lane) - 1u))) & (RING - 1);
+                 R[0][slot] = make_double2(w0, w1);
+                 R[1][slot] = make_double2(w2, -d2 * S.inv_radius);
+                 R[2][slot] = make_double2(zq.y, jv.x);
+                 R[3][slot] = make_double2(jv.y, jt.x);
+               }
+               count += __popc(bal);
+               __syncwarp();
+               if (count >= 32) {
+                 drain_full();
+                 __syncwarp();
+               }
+             });
   if (count > 0) drain(count);
   if (COUNT) {
 #pragma unroll
@@ -393,13 +470,15 @@ __global__ void __launch_bounds__(BLOCK, PRT_GATHER_MIN_BLOCKS)
       if (nevals) atomicAdd(&counters[2], nevals);
     }
   }
-  if (live) {
-    const long long u = p0 + lane;
-    out[u] = r0 + r1;
-    out[npos + u] = x0 + x1;
-    out[2 * npos + u] = y0 + y1;
-    out[3 * npos + u] = z0 + z1;
-  }
+#pragma unroll
+  for (int h = 0; h < PPL; ++h)
+    if (live[h]) {
+      const long long u = p0 + lane + 32 * h;
+      out[u] = r0[h] + r1[h];
+      out[npos + u] = x0[h] + x1[h];
+      out[2 * npos + u] = y0[h] + y1[h];
+      out[3 * npos + u] = z0[h] + z1[h];
+    }
 }
 
 // Mixed-precision form of deposit_groups_kernel: the same culling and order,
@@ -408,8 +487,8 @@ __global__ void __launch_bounds__(BLOCK, PRT_GATHER_MIN_BLOCKS)
 // and the contributions summed in FP32 over each batch of 32 ring entries,
 // then combined into FP64 per-position accumulators. A ring entry is 32
 // bytes: (wx, wy, wz, |w|^2), (qN, qN vx, qN vy, qN vz).
-template <bool ALPHA2>
-__global__ void __launch_bounds__(BLOCK, PRT_GATHER_MIN_BLOCKS)
+template <bool ALPHA2, int PPL = 1>
+__global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_MIXED_MIN_BLOCKS_WIDE)
     deposit_groups_mixed_kernel(const double *__restrict__ pos, long long ngroups,
                                 const uint32_t *__restrict__ gstarts,
                                 const double *__restrict__ gspheres, BinGrid G,
@@ -422,172 +501,122 @@ __global__ void __launch_bounds__(BLOCK, PRT_GATHER_MIN_BLOCKS)
   if (g >= ngroups) return;  // whole warp
   const uint32_t p0 = gstarts[g];
   const int npg = (int)(gstarts[g + 1] - p0);
-  const bool live = lane < npg;
   float4(*R)[RING] = ring[wid];
 
   const double c0 = gspheres[4 * g], c1 = gspheres[4 * g + 1], c2 = gspheres[4 * g + 2];
-  const double reach = S.radius + gspheres[4 * g + 3];
-  const double cull2 = (reach * (1 + 1e-9)) * (reach * (1 + 1e-9));
-  float U0 = 0, U1 = 0, U2 = 0, A = 0;
-  if (live) {
-    const long long u = p0 + lane;
-    const float u0 = (float)(pos[3 * u] - c0), u1 = (float)(pos[3 * u + 1] - c1),
-                u2 = (float)(pos[3 * u + 2] - c2);
-    A = u0 * u0 + u1 * u1 + u2 * u2;
-    U0 = -2 * u0;
-    U1 = -2 * u1;
-    U2 = -2 * u2;
+  // lane holds positions p0 + lane + 32 h, h < PPL; the weight base
+  // a - r^2/a = B + e + V . w as in deposit_groups_kernel, B and V rounded
+  // to FP32 from FP64
+  float V0[PPL], V1[PPL], V2[PPL], B[PPL];
+  bool live[PPL];
+#pragma unroll
+  for (int h = 0; h < PPL; ++h) {
+    live[h] = lane + 32 * h < npg;
+    V0[h] = V1[h] = V2[h] = B[h] = 0;
+    if (live[h]) {
+      const long long u = p0 + lane + 32 * h;
+      const double u0 = pos[3 * u] - c0, u1 = pos[3 * u + 1] - c1, u2 = pos[3 * u + 2] - c2;
+      B[h] = (float)(S.radius - (u0 * u0 + u1 * u1 + u2 * u2) * S.inv_radius);
+      V0[h] = (float)(2 * u0 * S.inv_radius);
+      V1[h] = (float)(2 * u1 * S.inv_radius);
+      V2[h] = (float)(2 * u2 * S.inv_radius);
+    }
   }
-  double r64 = 0, x64 = 0, y64 = 0, z64 = 0;
-  const float neg_inv_a = (float)-S.inv_radius, rad = (float)S.radius, alpha = (float)S.alpha;
-  auto weight = [&](float r2) -> float {
-    const float tr = fmaf(r2, neg_inv_a, rad);
+  double r64[PPL], x64[PPL], y64[PPL], z64[PPL];
+#pragma unroll
+  for (int h = 0; h < PPL; ++h) r64[h] = x64[h] = y64[h] = z64[h] = 0;
+  const float alpha = (float)S.alpha;
+  auto weight = [&](float tr) -> float {
     if (ALPHA2) {
       const float tp = fmaxf(tr, 0.0f);
       return tp * tp;
     }
     return tr > 0 ? powf(tr, alpha) : 0.0f;
   };
+  auto pair = [&](const float4 p, const float4 q, float *r, float *x, float *y, float *z) {
+#pragma unroll
+    for (int h = 0; h < PPL; ++h) {
+      const float sw = weight(fmaf(V0[h], p.x, fmaf(V1[h], p.y, fmaf(V2[h], p.z, B[h] + p.w))));
+      r[h] = fmaf(q.x, sw, r[h]);
+      x[h] = fmaf(q.y, sw, x[h]);
+      y[h] = fmaf(q.z, sw, y[h]);
+      z[h] = fmaf(q.w, sw, z[h]);
+    }
+  };
+  // FP32 batch sums into the FP64 accumulators
+  auto combine = [&](const float *ra, const float *xa, const float *ya, const float *za,
+                     const float *rb, const float *xb, const float *yb, const float *zb) {
+#pragma unroll
+    for (int h = 0; h < PPL; ++h) {
+      r64[h] += (double)ra[h] + (double)rb[h];
+      x64[h] += (double)xa[h] + (double)xb[h];
+      y64[h] += (double)ya[h] + (double)yb[h];
+      z64[h] += (double)za[h] + (double)zb[h];
+    }
+  };
   int head = 0, count = 0;
   auto drain = [&](int k) {
-    float ra = 0, xa = 0, ya = 0, za = 0, rb = 0, xb = 0, yb = 0, zb = 0;
-    int i = 0;
-    for (; i + 1 < k; i += 2) {
-      const int ea = (head + i) & (RING - 1), eb = (head + i + 1) & (RING - 1);
-      const float4 pa = R[0][ea], pb = R[0][eb];
-      const float r2a = fmaf(U0, pa.x, fmaf(U1, pa.y, fmaf(U2, pa.z, A + pa.w)));
-      const float r2b = fmaf(U0, pb.x, fmaf(U1, pb.y, fmaf(U2, pb.z, A + pb.w)));
-      const float sa = weight(r2a), sb = weight(r2b);
-      const float4 qa = R[1][ea], qb = R[1][eb];
-      ra = fmaf(qa.x, sa, ra);
-      xa = fmaf(qa.y, sa, xa);
-      ya = fmaf(qa.z, sa, ya);
-      za = fmaf(qa.w, sa, za);
-      rb = fmaf(qb.x, sb, rb);
-      xb = fmaf(qb.y, sb, xb);
-      yb = fmaf(qb.z, sb, yb);
-      zb = fmaf(qb.w, sb, zb);
+    float ra[PPL], xa[PPL], ya[PPL], za[PPL], rb[PPL], xb[PPL], yb[PPL], zb[PPL];
+#pragma unroll
+    for (int h = 0; h < PPL; ++h) ra[h] = xa[h] = ya[h] = za[h] = rb[h] = xb[h] = yb[h] = zb[h] = 0;
+    for (int i = 0; i < k; ++i) {
+      const int e = (head + i) & (RING - 1);
+      pair(R[0][e], R[1][e], ra, xa, ya, za);
     }
-    if (i < k) {
-      const int ea = (head + i) & (RING - 1);
-      const float4 pa = R[0][ea];
-      const float r2a = fmaf(U0, pa.x, fmaf(U1, pa.y, fmaf(U2, pa.z, A + pa.w)));
-      const float sa = weight(r2a);
-      const float4 qa = R[1][ea];
-      ra = fmaf(qa.x, sa, ra);
-      xa = fmaf(qa.y, sa, xa);
-      ya = fmaf(qa.z, sa, ya);
-      za = fmaf(qa.w, sa, za);
-    }
-    r64 += (double)ra + (double)rb;
-    x64 += (double)xa + (double)xb;
-    y64 += (double)ya + (double)yb;
-    z64 += (double)za + (double)zb;
+    combine(ra, xa, ya, za, rb, xb, yb, zb);
     head = (head + k) & (RING - 1);
     count -= k;
   };
+  // a full batch of 32 from head (0 or 32): constant offsets, two entries
+  // per step into two sets of FP32 batch sums
+  auto drain_full = [&]() {
+    float ra[PPL], xa[PPL], ya[PPL], za[PPL], rb[PPL], xb[PPL], yb[PPL], zb[PPL];
+#pragma unroll
+    for (int h = 0; h < PPL; ++h) ra[h] = xa[h] = ya[h] = za[h] = rb[h] = xb[h] = yb[h] = zb[h] = 0;
+    const float4 *E0 = &R[0][head], *E1 = &R[1][head];
+#pragma unroll MIXED_UNROLL
+    for (int i = 0; i < 32; i += 2) {
+      pair(E0[i], E1[i], ra, xa, ya, za);
+      pair(E0[i + 1], E1[i + 1], rb, xb, yb, zb);
+    }
+    combine(ra, xa, ya, za, rb, xb, yb, zb);
+    head = (head + 32) & (RING - 1);
+    count -= 32;
+  };
 
   const double cc[3] = {c0, c1, c2};
-  int ulo[3], uhi[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    ulo[d] = bin_floor(G, d, cc[d] - reach);
-    uhi[d] = bin_floor(G, d, cc[d] + reach);
-    if (G.periodic[d]) {
-      ulo[d] -= 1;
-      uhi[d] += 1;
-    } else {
-      ulo[d] = max(ulo[d], 0);
-      uhi[d] = min(uhi[d], G.dims[d] - 1);
-    }
-  }
-  const double reach_c = reach * (1 + 1e-6);
-  const double reach_c2 = reach_c * reach_c;
+  double blo[3], bhi[3];
+  warp_box<PPL>(pos, p0, npg, lane, cc, blo, bhi);
   const double2 *__restrict__ pay = reinterpret_cast<const double2 *>(P.payload);
-
-  for (int bz = ulo[2]; bz <= uhi[2]; ++bz) {
-    int wz = bz, qz = 0;
-    if (G.periodic[2]) { qz = floor_div(bz, G.dims[2]); wz = bz - qz * G.dims[2]; }
-    const double sz = qz * G.period[2] - c2;
-    double dz2;
-    {
-      const double blo = G.origin[2] + bz * G.w[2], bhi = blo + G.w[2];
-      const double e = fmax(0.0, fmax(blo - c2, c2 - bhi)) - G.slack[2];
-      dz2 = e > 0 ? e * e : 0.0;
-      if (dz2 > reach_c2) continue;
-    }
-    for (int by = ulo[1]; by <= uhi[1]; ++by) {
-      int wy = by, qy = 0;
-      if (G.periodic[1]) { qy = floor_div(by, G.dims[1]); wy = by - qy * G.dims[1]; }
-      const double sy = qy * G.period[1] - c1;
-      int bx0, bx1;
-      {
-        const double blo = G.origin[1] + by * G.w[1], bhi = blo + G.w[1];
-        const double e = fmax(0.0, fmax(blo - c1, c1 - bhi)) - G.slack[1];
-        const double dyz2 = dz2 + (e > 0 ? e * e : 0.0);
-        if (dyz2 > reach_c2) continue;
-        const double rem = sqrt(reach_c2 - dyz2);
-        bx0 = bin_floor(G, 0, c0 - rem);
-        bx1 = bin_floor(G, 0, c0 + rem);
-        if (G.periodic[0]) {
-          bx0 -= 1;
-          bx1 += 1;
-        }
-        bx0 = max(bx0, ulo[0]);
-        bx1 = min(bx1, uhi[0]);
-      }
-      int bx = bx0;
-      while (bx <= bx1) {
-        int wx = bx, qx = 0, seg_end = bx1;
-        if (G.periodic[0]) {
-          qx = floor_div(bx, G.dims[0]);
-          wx = bx - qx * G.dims[0];
-          seg_end = min(bx1, (qx + 1) * G.dims[0] - 1);
-        }
-        const double sx = qx * G.period[0] - c0;
-        const long long row = (long long)G.dims[0] * (wy + (long long)G.dims[1] * wz);
-        const uint32_t s0 = P.starts[row + wx];
-        const uint32_t s1 = P.starts[row + wx + (seg_end - bx) + 1];
-        bx = seg_end + 1;
-        for (uint32_t b0 = s0; b0 < s1; b0 += 32) {
-          const uint32_t k = b0 + lane;
-          bool in = false;
-          double w0 = 0, w1 = 0, w2 = 0, d2 = 0, qn = 0;
-          if (k < s1) {
-            const double2 xy = pay[4 * (size_t)k], zq = pay[4 * (size_t)k + 1];
-            w0 = xy.x + sx;
-            w1 = xy.y + sy;
-            w2 = zq.x + sz;
-            qn = zq.y;
-            d2 = w0 * w0 + w1 * w1 + w2 * w2;
-            in = d2 <= cull2;
-          }
-          const unsigned bal = __ballot_sync(0xffffffffu, in);
-          if (in) {
-            const double2 jv = pay[4 * (size_t)k + 2], jt = pay[4 * (size_t)k + 3];
-            const int slot = (head + count + __popc(bal & ((1u << lane) - 1u))) & (RING - 1);
-            const float f0 = (float)w0, f1 = (float)w1, f2 = (float)w2;
-            R[0][slot] = make_float4(f0, f1, f2, f0 * f0 + f1 * f1 + f2 * f2);
-            R[1][slot] = make_float4((float)qn, (float)jv.x, (float)jv.y, (float)jt.x);
-          }
-          count += __popc(bal);
-          __syncwarp();
-          if (count >= 32) {
-            drain(32);
-            __syncwarp();
-          }
-        }
-      }
-    }
-  }
+  stream_box(G, P, cc, blo, bhi, S.radius, lane,
+             [&](bool in, uint32_t k, double w0, double w1, double w2, double d2) {
+               const unsigned bal = __ballot_sync(0xffffffffu, in);
+               if (in) {
+                 const double2 zq = pay[4 * (size_t)k + 1];
+                 const double2 jv = pay[4 * (size_t)k + 2], jt = pay[4 * (size_t)k + 3];
+                 const int slot =
+                     (head + count + __popc(bal & ((1u << lane) - 1u))) & (RING - 1);
+                 R[0][slot] = make_float4((float)w0, (float)w1, (float)w2,
+                                          (float)(-d2 * S.inv_radius));
+                 R[1][slot] = make_float4((float)zq.y, (float)jv.x, (float)jv.y, (float)jt.x);
+               }
+               count += __popc(bal);
+               __syncwarp();
+               if (count >= 32) {
+                 drain_full();
+                 __syncwarp();
+               }
+             });
   if (count > 0) drain(count);
-  if (live) {
-    const long long u = p0 + lane;
-    out[u] = r64;
-    out[npos + u] = x64;
-    out[2 * npos + u] = y64;
-    out[3 * npos + u] = z64;
-  }
+#pragma unroll
+  for (int h = 0; h < PPL; ++h)
+    if (live[h]) {
+      const long long u = p0 + lane + 32 * h;
+      out[u] = r64[h];
+      out[npos + u] = x64[h];
+      out[2 * npos + u] = y64[h];
+      out[3 * npos + u] = z64[h];
+    }
 }
 
 // Every node takes the values of its position.
@@ -830,34 +859,50 @@ int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
     int level = (int)std::lround(std::log2(ext / side));
     level = std::min(std::max(level, 0), 21);
     const int shift = 3 * (21 - level);
-    std::vector<uint32_t> gstart;
-    gstart.reserve(npos / 16 + 2);
-    uint64_t prev_cell = ~0ull;
-    for (long long u = 0; u < npos; ++u) {
-      const uint64_t cell = key[order[run_starts[u]]] >> shift;
-      if (u == 0 || cell != prev_cell || u - gstart.back() >= PRT_WARP_NODES)
-        gstart.push_back((uint32_t)u);
-      prev_cell = cell;
-    }
-    gstart.push_back((uint32_t)npos);
-    const long long groups = (long long)gstart.size() - 1;
-    std::vector<double> spheres(4 * (size_t)std::max<long long>(1, groups));
-    for (long long g = 0; g < groups; ++g) {
-      double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-      for (uint32_t p = gstart[g]; p < gstart[g + 1]; ++p)
-        for (int a = 0; a < 3; ++a) {
-          lo[a] = std::min(lo[a], pos[3 * p + a]);
-          hi[a] = std::max(hi[a], pos[3 * p + a]);
-        }
-      double c[3], r2 = 0;
-      for (int a = 0; a < 3; ++a) c[a] = 0.5 * (lo[a] + hi[a]);
-      for (uint32_t p = gstart[g]; p < gstart[g + 1]; ++p) {
-        double s = 0;
-        for (int a = 0; a < 3; ++a) s += (pos[3 * p + a] - c[a]) * (pos[3 * p + a] - c[a]);
-        r2 = std::max(r2, s);
+    // runs of <= maxlen positions cut at Morton cells (key >> cell_shift),
+    // with their bounding spheres
+    auto build_groups = [&](int cell_shift, long long maxlen, std::vector<uint32_t> &gs,
+                            std::vector<double> &sph) {
+      gs.clear();
+      gs.reserve(npos / 16 + 2);
+      uint64_t prev_cell = ~0ull;
+      for (long long u = 0; u < npos; ++u) {
+        const uint64_t cell = key[order[run_starts[u]]] >> cell_shift;
+        if (u == 0 || cell != prev_cell || u - gs.back() >= maxlen) gs.push_back((uint32_t)u);
+        prev_cell = cell;
       }
-      for (int a = 0; a < 3; ++a) spheres[4 * g + a] = c[a];
-      spheres[4 * g + 3] = std::sqrt(r2) * (1 + 1e-9) + 1e-300;
+      gs.push_back((uint32_t)npos);
+      const long long ng = (long long)gs.size() - 1;
+      sph.assign(4 * (size_t)std::max<long long>(1, ng), 0.0);
+      for (long long g = 0; g < ng; ++g) {
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (uint32_t p = gs[g]; p < gs[g + 1]; ++p)
+          for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], pos[3 * p + a]);
+            hi[a] = std::max(hi[a], pos[3 * p + a]);
+          }
+        double c[3], r2 = 0;
+        for (int a = 0; a < 3; ++a) c[a] = 0.5 * (lo[a] + hi[a]);
+        for (uint32_t p = gs[g]; p < gs[g + 1]; ++p) {
+          double s = 0;
+          for (int a = 0; a < 3; ++a) s += (pos[3 * p + a] - c[a]) * (pos[3 * p + a] - c[a]);
+          r2 = std::max(r2, s);
+        }
+        for (int a = 0; a < 3; ++a) sph[4 * g + a] = c[a];
+        sph[4 * g + 3] = std::sqrt(r2) * (1 + 1e-9) + 1e-300;
+      }
+    };
+    std::vector<uint32_t> gstart;
+    std::vector<double> spheres;
+    build_groups(shift, PRT_WARP_NODES, gstart, spheres);
+    const long long groups = (long long)gstart.size() - 1;
+    {
+      std::vector<uint32_t> wstart;
+      std::vector<double> wsph;
+      build_groups(std::min(shift + PRT_WIDE_CELL_BITS, 63), 2 * PRT_WARP_NODES, wstart, wsph);
+      P.wide_groups = (long long)wstart.size() - 1;
+      if ((rc = upload_vec(wstart, &P.wide_starts))) return rc;
+      if ((rc = upload_vec(wsph, &P.wide_spheres))) return rc;
     }
     P.groups = groups;
     if ((rc = upload_vec(gstart, &P.group_starts))) return rc;
@@ -1056,31 +1101,41 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
   if (!vals) return rc;
   {
     ScopedTimer timer(ws, PRT_TIME_DEPOSIT_GATHER, s);
-    const unsigned nb = (unsigned)((PS.groups + WARPS - 1) / WARPS);
+    auto groups_for = [&](int ppl, long long &ng, const uint32_t *&gs, const double *&gsp) {
+      ng = ppl == 2 ? PS.wide_groups : PS.groups;
+      gs = ppl == 2 ? PS.wide_starts : PS.group_starts;
+      gsp = ppl == 2 ? PS.wide_spheres : PS.group_spheres;
+      return (unsigned)((ng + WARPS - 1) / WARPS);
+    };
+    long long ng;
+    const uint32_t *gs;
+    const double *gsp;
     if (precision == PRT_PRECISION_MIXED) {
+      constexpr int W = PRT_MIXED_PPL;
+      const unsigned nb = groups_for(W, ng, gs, gsp);
       if (a2)
-        deposit_groups_mixed_kernel<true><<<nb, BLOCK, 0, s>>>(
-            PS.pos, PS.groups, PS.group_starts, PS.group_spheres, G, P, S, PS.count, vals);
+        deposit_groups_mixed_kernel<true, W><<<nb, BLOCK, 0, s>>>(PS.pos, ng, gs, gsp, G, P, S,
+                                                                  PS.count, vals);
       else
-        deposit_groups_mixed_kernel<false><<<nb, BLOCK, 0, s>>>(
-            PS.pos, PS.groups, PS.group_starts, PS.group_spheres, G, P, S, PS.count, vals);
-    } else if (counter) {
-      if (a2)
-        deposit_groups_kernel<true, true><<<nb, BLOCK, 0, s>>>(
-            PS.pos, PS.groups, PS.group_starts, PS.group_spheres, PS.run_starts, G, P, S,
-            PS.count, vals, counter);
-      else
-        deposit_groups_kernel<false, true><<<nb, BLOCK, 0, s>>>(
-            PS.pos, PS.groups, PS.group_starts, PS.group_spheres, PS.run_starts, G, P, S,
-            PS.count, vals, counter);
-    } else if (a2) {
-      deposit_groups_kernel<true, false><<<nb, BLOCK, 0, s>>>(
-          PS.pos, PS.groups, PS.group_starts, PS.group_spheres, PS.run_starts, G, P, S,
-          PS.count, vals, nullptr);
+        deposit_groups_mixed_kernel<false, W><<<nb, BLOCK, 0, s>>>(PS.pos, ng, gs, gsp, G, P, S,
+                                                                   PS.count, vals);
     } else {
-      deposit_groups_kernel<false, false><<<nb, BLOCK, 0, s>>>(
-          PS.pos, PS.groups, PS.group_starts, PS.group_spheres, PS.run_starts, G, P, S,
-          PS.count, vals, nullptr);
+      constexpr int W = PRT_FP64_PPL;
+      const unsigned nb = groups_for(W, ng, gs, gsp);
+      if (counter) {
+        if (a2)
+          deposit_groups_kernel<true, true, W><<<nb, BLOCK, 0, s>>>(
+              PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, counter);
+        else
+          deposit_groups_kernel<false, true, W><<<nb, BLOCK, 0, s>>>(
+              PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, counter);
+      } else if (a2) {
+        deposit_groups_kernel<true, false, W><<<nb, BLOCK, 0, s>>>(
+            PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, nullptr);
+      } else {
+        deposit_groups_kernel<false, false, W><<<nb, BLOCK, 0, s>>>(
+            PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, nullptr);
+      }
     }
     PRT_CHECK_CUDA(cudaGetLastError());
   }

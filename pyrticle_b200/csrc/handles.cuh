@@ -49,6 +49,12 @@ struct PositionSet {
   long long groups = 0;
   const uint32_t *group_starts = nullptr; // [groups + 1]
   const double *group_spheres = nullptr;  // [groups][4]: centre xyz, radius
+  // wide warp groups for the deposition (two positions per lane): runs of
+  // <= 64 positions that never straddle a Morton cell of about twice the
+  // group target
+  long long wide_groups = 0;
+  const uint32_t *wide_starts = nullptr;  // [wide_groups + 1]
+  const double *wide_spheres = nullptr;   // [wide_groups][4]
   // the groups binned by the bin of their sphere centre (each group in
   // exactly one bin; uniform bins of about a group radius), in bin order:
   // spheres and position ranges, with CSR bin starts
@@ -109,6 +115,11 @@ constexpr int PRT_NODE_TILE = 128;
 constexpr int PRT_WARP_NODES = 32;
 // target positions per Morton cell when cutting warp groups
 constexpr double PRT_GROUP_TARGET = 24.0;
+// Morton bits dropped from the group cells for the wide groups (1: cells of
+// two sibling cells, about twice the positions)
+#ifndef PRT_WIDE_CELL_BITS
+#define PRT_WIDE_CELL_BITS 1
+#endif
 
 void *ws_buffer(prt_workspace *ws, int slot, size_t bytes, int *rc);
 int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d);
