@@ -233,6 +233,12 @@ __device__ __forceinline__ void stream_box(const BinGrid &G, const DepParticles 
     }
   }
   const double2 *__restrict__ pay = reinterpret_cast<const double2 *>(P.payload);
+  double mid[3], half[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    mid[d] = 0.5 * (lo[d] + hi[d]);
+    half[d] = 0.5 * (hi[d] - lo[d]);
+  }
   // distance from the slab [blo, blo + w) of bins to the box along one axis
   auto slab_gap = [&](int d, double blo) {
     const double e = fmax(0.0, fmax(blo - (c[d] + hi[d]), (c[d] + lo[d]) - (blo + G.w[d]))) -
@@ -283,10 +289,12 @@ __device__ __forceinline__ void stream_box(const BinGrid &G, const DepParticles 
             w1 = xy.y + sy;
             w2 = zq.x + sz;
             d2 = w0 * w0 + w1 * w1 + w2 * w2;
-            const double e0 = fmax(0.0, fmax(lo[0] - w0, w0 - hi[0]));
-            const double e1 = fmax(0.0, fmax(lo[1] - w1, w1 - hi[1]));
-            const double e2 = fmax(0.0, fmax(lo[2] - w2, w2 - hi[2]));
-            in = e0 * e0 + e1 * e1 + e2 * e2 <= rc2;
+            // per axis 2 max(|w - mid| - half, 0) = d + |d|
+            const double d0 = fabs(w0 - mid[0]) - half[0];
+            const double d1 = fabs(w1 - mid[1]) - half[1];
+            const double d2a = fabs(w2 - mid[2]) - half[2];
+            const double e0 = d0 + fabs(d0), e1 = d1 + fabs(d1), e2 = d2a + fabs(d2a);
+            in = e0 * e0 + e1 * e1 + e2 * e2 <= 4 * rc2;
           }
           visit(in, k, w0, w1, w2, d2);
         }
@@ -383,13 +391,17 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
   unsigned long long npairs = 0, nnode = 0, nevals = 0;
 
   // shape weight from tr = a - r^2/a (zero beyond the radius)
+  // alpha = 2: (tr + |tr|)^2 = 4 max(tr, 0)^2 exactly (one add with an
+  // absolute-value operand and one multiply); the sums are scaled by 1/4 at
+  // the end, also exactly, so the result equals that of max(tr, 0)^2
   auto weight = [&](double tr) -> double {
     if (ALPHA2) {
-      const double tp = fmax(tr, 0.0);
-      return tp * tp;
+      const double t2 = tr + fabs(tr);
+      return t2 * t2;
     }
     return tr > 0 ? pow(tr, S.alpha) : 0.0;
   };
+  const double wscale = ALPHA2 ? 0.25 : 1.0;
   // one ring entry against the lane's positions
   auto pair = [&](const double2 p, const double2 q, const double2 wq, const double2 wv,
                   double *r, double *x, double *y, double *z) {
@@ -474,10 +486,10 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
   for (int h = 0; h < PPL; ++h)
     if (live[h]) {
       const long long u = p0 + lane + 32 * h;
-      out[u] = r0[h] + r1[h];
-      out[npos + u] = x0[h] + x1[h];
-      out[2 * npos + u] = y0[h] + y1[h];
-      out[3 * npos + u] = z0[h] + z1[h];
+      out[u] = (r0[h] + r1[h]) * wscale;
+      out[npos + u] = (x0[h] + x1[h]) * wscale;
+      out[2 * npos + u] = (y0[h] + y1[h]) * wscale;
+      out[3 * npos + u] = (z0[h] + z1[h]) * wscale;
     }
 }
 
@@ -526,13 +538,16 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
 #pragma unroll
   for (int h = 0; h < PPL; ++h) r64[h] = x64[h] = y64[h] = z64[h] = 0;
   const float alpha = (float)S.alpha;
+  // alpha = 2: (tr + |tr|)^2 = 4 max(tr, 0)^2, the 1/4 applied to the FP64
+  // sums at the end (exact)
   auto weight = [&](float tr) -> float {
     if (ALPHA2) {
-      const float tp = fmaxf(tr, 0.0f);
-      return tp * tp;
+      const float t2 = tr + fabsf(tr);
+      return t2 * t2;
     }
     return tr > 0 ? powf(tr, alpha) : 0.0f;
   };
+  const double wscale = ALPHA2 ? 0.25 : 1.0;
   auto pair = [&](const float4 p, const float4 q, float *r, float *x, float *y, float *z) {
 #pragma unroll
     for (int h = 0; h < PPL; ++h) {
@@ -612,10 +627,10 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
   for (int h = 0; h < PPL; ++h)
     if (live[h]) {
       const long long u = p0 + lane + 32 * h;
-      out[u] = r64[h];
-      out[npos + u] = x64[h];
-      out[2 * npos + u] = y64[h];
-      out[3 * npos + u] = z64[h];
+      out[u] = r64[h] * wscale;
+      out[npos + u] = x64[h] * wscale;
+      out[2 * npos + u] = y64[h] * wscale;
+      out[3 * npos + u] = z64[h] * wscale;
     }
 }
 
