@@ -45,7 +45,6 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adjoint-scale", type=float, default=1.0,
                     help="particle-count scale of the differentiable workload (1M electrons)")
@@ -169,6 +168,70 @@ def fp64_peak_tflops(torch):
         best = min(best, e0.elapsed_time(e1))
     del a, b
     return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def fp32_peak_tflops(torch):
+    """FP32 CUDA-core peak measured here: cuBLAS SGEMM 8192^3 with TF32 off."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        best = 1e9
+        for _ in range(5):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def form_accuracy(m, s, fields, dt, torch, steps=5):
+    """Errors of the chosen form against the plain FP64 form on the same
+    state: one deposition (rho, j), the first stage's residual kp = dt F
+    (forces), and positions / momentum changes after `steps` steps."""
+    from pyrticle_b200 import _lib
+    from pyrticle_b200.cloud import LSRK4_A, LSRK4_B
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))  # noqa: E731
+    r64, j64 = m.depositor.deposit_densities_device(s, precision="fp64")
+    r32, j32 = m.depositor.deposit_densities_device(s, precision="mixed")
+    out = {"rho_rel_l2": rel(r32, r64), "j_rel_l2": rel(j32, j64)}
+    del r64, j64, r32, j32
+    fp = m.pusher.field_pointers(fields)
+    c = m.units.VACUUM_LIGHT_SPEED()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def run(prec, stages):
+        x, p, el = s.x.clone(), s.p.clone(), s.el.clone()
+        kx = torch.zeros_like(x)
+        kp = torch.zeros_like(p)
+        for t in range(stages):
+            _lib.check(m.lib.prt_lsrk_stage(
+                m.pusher.handle, m.workspace, x.shape[1], x.data_ptr(), p.data_ptr(),
+                s.q.data_ptr(), s.m.data_ptr(), el.data_ptr(), kx.data_ptr(), kp.data_ptr(), fp,
+                LSRK4_A[t % 5], LSRK4_B[t % 5], dt, c, prec, stream))
+        return x, p, el, kp
+
+    kp64 = run(0, 1)[3]
+    kp32 = run(1, 1)[3]
+    out["force_rel_l2"] = rel(kp32, kp64)
+    del kp64, kp32
+    x64, p64, el64, _ = run(0, 5 * steps)
+    x32, p32, el32, _ = run(1, 5 * steps)
+    out[f"x_rel_l2_after_{steps}_steps"] = rel(x32, x64)
+    out[f"dp_rel_l2_after_{steps}_steps"] = rel(p32 - s.p, p64 - s.p)
+    out["elements_equal_fraction"] = float((el32 == el64).float().mean())
+    m.check_status()
+    return out
 
 
 def cpu_baseline(w, target_seconds, threads=0, steps=1, seed=7):
@@ -354,17 +417,13 @@ def main():
     n = len(s)
     nn = len(m.discretization)
 
-    def one_step():
-        rho, j = m.step(s, fields, w.dt, steps=1, check=False)
-        if world > 1:
-            dist.all_reduce(rho)
-            dist.all_reduce(j)
-        return rho, j
+    prec = {"fp64": 0, "mixed": 1}
 
-    def one_step_mixed():
-        m.depositor.precision = "mixed"
+    def one_step(form):
+        """One step of the given form: 5 fused RK stages + the deposition."""
+        m.depositor.precision = form
         try:
-            rho, j = m.step(s, fields, w.dt, steps=1, check=False)
+            rho, j = m.step(s, fields, w.dt, steps=1, check=False, precision=prec[form])
         finally:
             m.depositor.precision = "fp64"
         if world > 1:
@@ -372,79 +431,50 @@ def main():
             dist.all_reduce(j)
         return rho, j
 
-    for _ in range(args.warmup):
-        one_step()
+    for form in ("fp64", "mixed"):
+        for _ in range(args.warmup):
+            one_step(form)
     torch.cuda.synchronize()
     pairs, node_pairs, evaluated = count_pairs(m, s, sf)
+    accuracy = form_accuracy(m, s, fields, w.dt, torch)
 
-    # ---- timed region (device events, max over ranks) ----
     clocks = ClockSampler(local)
-    _lib.check(m.lib.prt_workspace_timing(m.workspace, 1))
-    for cat in range(4):
-        timing_read(m, cat, reset=True)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
     clocks.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        one_step()
-    e1.record()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    _lib.check(m.lib.prt_workspace_timing(m.workspace, 0))
-    ms = e0.elapsed_time(e1)
-    kernel = {name: timing_read(m, cat) for cat, name in
-              enumerate(("deposit_gather", "deposit_stage", "lsrk_stage", "sort"))}
-    m.check_status()
-    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
-    value = world * n * args.steps / (ms * 1e-3)
 
-    # ---- the mixed-precision form on the same workload ----
-    mixed = None
-    if not args.no_mixed:
-        # accuracy: one deposition of the same store in both forms
-        r64, j64 = m.depositor.deposit_densities_device(s, precision="fp64")
-        r32, j32 = m.depositor.deposit_densities_device(s, precision="mixed")
-        err_rho = float(torch.linalg.norm(r32 - r64) / torch.linalg.norm(r64))
-        err_j = float(torch.linalg.norm(j32 - j64) / torch.linalg.norm(j64))
-        for _ in range(args.warmup):
-            one_step_mixed()
+    def timed(form):
+        """K timed steps of one form (device events, max over ranks) with the
+        per-category kernel times."""
         _lib.check(m.lib.prt_workspace_timing(m.workspace, 1))
-        timing_read(m, 0, reset=True)
+        for cat in range(4):
+            timing_read(m, cat, reset=True)
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        g0 = torch.cuda.Event(enable_timing=True)
-        g1 = torch.cuda.Event(enable_timing=True)
-        g0.record()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
         for _ in range(args.steps):
-            one_step_mixed()
-        g1.record()
+            one_step(form)
+        e1.record()
         torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
         _lib.check(m.lib.prt_workspace_timing(m.workspace, 0))
-        mms = g0.elapsed_time(g1)
-        mg, mk = timing_read(m, 0)
-        t = torch.tensor([mms], device="cuda", dtype=torch.float64)
+        t = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        mms = float(t.item())
-        mixed = {"value": world * n * args.steps / (mms * 1e-3), "unit": METRIC,
-                 "ms_per_step": mms / args.steps,
-                 "deposit_ms_per_step": mg / args.steps,
-                 "speedup_vs_fp64": ms / mms,
-                 "rho_rel_l2_vs_fp64": err_rho, "j_rel_l2_vs_fp64": err_j,
-                 "form": "shape weights and 32-particle batch sums in FP32, FP64 "
-                         "per-node combine; push, interpolation and locate FP64"}
+        kernel = {name: timing_read(m, cat) for cat, name in
+                  enumerate(("deposit_gather", "deposit_stage", "lsrk_stage", "sort"))}
+        return float(t.item()), kernel
 
-    # ---- end to end: host buffers through the same API ----
+    ms64, kernel64 = timed("fp64")
+    ms, kernel = timed("mixed")
+    clk = clocks.stop()
+    m.check_status()
+    value = world * n * args.steps / (ms * 1e-3)
+    value64 = world * n * args.steps / (ms64 * 1e-3)
+
+    # ---- end to end: host buffers through the same API (chosen form) ----
     e2e = None
     if not args.no_e2e:
         hx = torch.empty_like(s.x, device="cpu").pin_memory()
@@ -471,7 +501,7 @@ def main():
             s.q.copy_(hq, non_blocking=True)
             s.m.copy_(hm, non_blocking=True)
             s.el.copy_(he, non_blocking=True)
-            rho, j = one_step()
+            rho, j = one_step("mixed")
             hrho.copy_(rho, non_blocking=True)
             hj.copy_(j, non_blocking=True)
         f1.record()
@@ -492,53 +522,69 @@ def main():
 
     peaks, src = measured_peaks()
     fp64 = fp64_peak_tflops(torch)
+    fp32 = fp32_peak_tflops(torch)
+    # dominant kernel of each form: the deposition gather, 15 flops per
+    # (particle, distinct position) pair within the radius
     gms, gk = kernel["deposit_gather"]
     avg_gather = gms / max(gk, 1)
-    flops_per_launch = 15.0 * pairs
-    achieved = flops_per_launch / (avg_gather * 1e-3) / 1e12
+    achieved = 15.0 * pairs / (avg_gather * 1e-3) / 1e12
+    gms64, gk64 = kernel64["deposit_gather"]
+    avg_gather64 = gms64 / max(gk64, 1)
+    achieved64 = 15.0 * pairs / (avg_gather64 * 1e-3) / 1e12
     sms, sk = kernel["lsrk_stage"]
-    stage_bytes = 216.0 * n
-    stage_gbs = stage_bytes / (sms / max(sk, 1) * 1e-3) / 1e9
-    roofline = {"bound": "fp64", "kernel": "deposit_groups_kernel (deposition)",
-                "achieved": achieved, "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
+    stage_gbs = 216.0 * n / (sms / max(sk, 1) * 1e-3) / 1e9
+    algorithmic = (f"15 flops x {pairs} (particle, distinct node position) pairs within the "
+                   f"radius per launch ({node_pairs} (particle, node) pairs over all DG nodes; "
+                   f"coincident nodes are evaluated once; {evaluated} pairs evaluated after "
+                   f"culling)")
+    roofline = {"bound": "fp32", "kernel": "deposit_groups_mixed_kernel (deposition, chosen form)",
+                "achieved": achieved, "peak": fp32, "unit": "TFLOP/s", "frac": achieved / fp32,
                 "traffic": None,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 pipe; "
-                               "MEASURED_PEAKS.json has no FP64 figure)",
-                "algorithmic": f"15 flops x {pairs} (particle, distinct node position) "
-                               f"pairs within the radius per launch ({node_pairs} "
-                               f"(particle, node) pairs over all DG nodes; coincident "
-                               f"nodes are evaluated once); {avg_gather:.3f} ms per launch",
-                "secondary": {"bound": "hbm", "kernel": "lsrk_stage_kernel<3>",
+                "peak_source": "cuBLAS SGEMM 8192^3 (TF32 off) measured in this run (FP32 "
+                               "pipe; MEASURED_PEAKS.json has no FP32 figure)",
+                "algorithmic": algorithmic + f"; {avg_gather:.3f} ms per launch",
+                "secondary": {"bound": "hbm", "kernel": "lsrk_stage_mixed_kernel<3>",
                               "achieved": stage_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                               "frac": stage_gbs / peaks["hbm_gbs"],
                               "algorithmic": "216 B per particle per stage",
                               "peak_source": src}}
+    fp64_block = {
+        "value": value64, "unit": METRIC, "ms_per_step": ms64 / args.steps,
+        "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kernel64.items()},
+        "roofline": {"bound": "fp64", "kernel": "deposit_groups_kernel (deposition, FP64)",
+                     "achieved": achieved64, "peak": fp64, "unit": "TFLOP/s",
+                     "frac": achieved64 / fp64, "traffic": None,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                     "algorithmic": algorithmic + f"; {avg_gather64:.3f} ms per launch"},
+        "form": "plain form: FP64 throughout"}
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64 (mixed: FP32 deposition, split-BF16 tensor-core Lagrange "
+                     "values, FP64 state/force/locate/combine)",
             "data": "synthetic (seeded mesh, particles and fields of the workload)",
             "config": {"workload": f"{args.workload}: {w.mesh.element_count} tets order "
                                    f"{w.order}, {n} particles/GPU, shape radius "
-                                   f"{w.shape_radius * 100:g} cm, FP64 plain form",
+                                   f"{w.shape_radius * 100:g} cm, chosen (mixed) form",
                        "particles_per_gpu": n, "elements": w.mesh.element_count,
-                       "nodes": nn, "order": w.order, "form": "fp64",
+                       "nodes": nn, "order": w.order, "form": "mixed",
                        "l2": "inputs larger than L2 (3.5 GB particle state per stage)",
                        "parallelism": f"particles sharded over {world} GPU(s), NCCL "
                                       "all-reduce of rho/j" if world > 1 else "1 GPU"},
             "clocks": clk, "gpu_launches": None, "roofline": roofline,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kernel.items()},
             "pairs_per_deposition": {"positions": pairs, "nodes": node_pairs,
-                                     "evaluated": evaluated}}
-    # libprt's own kernels in the timed region (CUB's radix-sort kernels not
-    # counted): per sort iota + 7 permutation gathers; per RK stage one fused
-    # kernel; per deposition bin keys, bin starts, payload, the gather and
-    # the expansion to nodes.
+                                     "evaluated": evaluated},
+            "fp64": fp64_block, "speedup_mixed_vs_fp64": ms64 / ms,
+            "accuracy_mixed_vs_fp64": accuracy}
+    # libprt's own kernels in the timed region of the headline form (CUB's
+    # radix-sort kernels not counted): per sort iota + 7 permutation gathers;
+    # per RK stage one fused kernel; per deposition bin keys, bin starts,
+    # payload, the gather and the expansion to nodes.
     line["gpu_launches"] = int(kernel["lsrk_stage"][1] + 2 * kernel["deposit_gather"][1] +
                                3 * kernel["deposit_stage"][1] + 8 * kernel["sort"][1])
     if e2e:
         line["e2e"] = e2e
-    if mixed:
-        line["mixed"] = mixed
     if not args.no_adjoint and world == 1:
         line["adjoint"] = adjoint_bench(torch, args.adjoint_scale, peaks["hbm_gbs"])
     if not args.no_cpu_baseline and world == 1:

@@ -40,7 +40,9 @@ enum prt_status {
   /* a particle handed to a kernel has no containing element */
   PRT_ERR_NOT_LOCATED = -5,
   /* scratch larger than a fixed-capacity entry point supports */
-  PRT_ERR_CAPACITY = -6
+  PRT_ERR_CAPACITY = -6,
+  /* a kernel's bounded wait on its own tensor-core work ran out */
+  PRT_ERR_TIMEOUT = -7
 };
 
 /* Warnings recorded in the status word (the reference WARNs, tools.hpp:467-508). */

@@ -25,6 +25,7 @@ ERRORS = {
     -4: "no best normal found--weird",
     -5: "particle has no containing element",
     -6: "size exceeds the fixed scratch capacity",
+    -7: "a kernel's bounded wait on its tensor-core work timed out",
 }
 PRT_WARN_ZERO_MASS = 1
 PRT_ERR_CAPACITY = -6

@@ -287,9 +287,19 @@ class DifferentiableTrajectory:
                 continue
             g = graphs.get(T)
             if g is None:
+                # captured on a side stream with capture_begin/capture_end:
+                # the torch.cuda.graph context would also empty the caching
+                # allocator, making every later allocation a cudaMalloc
                 g = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(g):
-                    segment(T)
+                side = torch.cuda.Stream()
+                side.wait_stream(torch.cuda.current_stream())
+                with torch.cuda.stream(side):
+                    g.capture_begin()
+                    try:
+                        segment(T)
+                    finally:
+                        g.capture_end()
+                torch.cuda.current_stream().wait_stream(side)
                 graphs[T] = g
             g.replay()
         meth.check_status()

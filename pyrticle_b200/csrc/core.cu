@@ -496,11 +496,17 @@ extern "C" int prt_monomial_pusher_create(const prt_mesh *mesh, int32_t np,
   P->w.assign((size_t)np * np, 0.0);
   for (int i = 0; i < np; ++i)
     for (int k = 0; k < np; ++k) P->w[(size_t)i * np + canon[k]] = Vinv[(size_t)k * np + i];
+  int rc = prt_pusher_prepare_mixed(P);
+  if (rc) {
+    delete P;
+    return rc;
+  }
   *out = P;
   return PRT_OK;
 }
 
 extern "C" int prt_monomial_pusher_destroy(prt_pusher *p) {
+  if (p && p->w_split) cudaFree(p->w_split);
   delete p;
   return PRT_OK;
 }
@@ -552,12 +558,17 @@ extern "C" int prt_lsrk_stage(const prt_pusher *P, prt_workspace *ws, int64_t n,
                               uint32_t *el, double *kx, double *kp,
                               const double *const fields[6], double a, double b,
                               double dt, double c, int32_t precision, void *stream) {
-  if (!P || !ws || n < 0 || !fields || precision != 0) return PRT_ERR_INVALID_ARGUMENT;
+  if (!P || !ws || n < 0 || !fields) return PRT_ERR_INVALID_ARGUMENT;
+  if (precision != PRT_PRECISION_FP64 && precision != PRT_PRECISION_MIXED)
+    return PRT_ERR_INVALID_ARGUMENT;
+  if (precision == PRT_PRECISION_MIXED && !P->w_split) return PRT_ERR_INVALID_ARGUMENT;
   if (n > 0 && (!x || !p || !q || !m || !el || !kx || !kp)) return PRT_ERR_INVALID_ARGUMENT;
   if (n == 0) return PRT_OK;
   Fields6 F;
   for (int k = 0; k < 6; ++k) F.f[k] = fields[k];
   cudaStream_t s = (cudaStream_t)stream;
+  if (precision == PRT_PRECISION_MIXED)
+    return launch_stage_mixed(P, ws, n, x, p, q, m, el, kx, kp, F, a, b, dt, c, s);
   switch (P->order) {
     case 1: return launch_stage<1>(P, ws, n, x, p, q, m, el, kx, kp, F, a, b, dt, c, s);
     case 2: return launch_stage<2>(P, ws, n, x, p, q, m, el, kx, kp, F, a, b, dt, c, s);

@@ -109,7 +109,19 @@ struct prt_pusher {
   int order;
   int np;
   std::vector<double> w;  // [np][np], canonical monomial order
+  // the mixed-precision stage's tensor-core operand: W rounded to FP32 and
+  // split into three BF16 terms, in the MMA's shared-memory layout (device)
+  void *w_split = nullptr;
 };
+
+// Builds prt_pusher::w_split (orders 1-3; a no-op for order 4).
+int prt_pusher_prepare_mixed(prt_pusher *P);
+// The mixed-precision stage (prt_lsrk_stage with PRT_PRECISION_MIXED).
+struct Fields6;
+int launch_stage_mixed(const prt_pusher *P, prt_workspace *ws, long long n, double *x,
+                       double *p, const double *q, const double *m, uint32_t *el, double *kx,
+                       double *kp, const Fields6 &F, double a, double b, double dt, double c,
+                       cudaStream_t s);
 
 constexpr int PRT_NODE_TILE = 128;
 constexpr int PRT_WARP_NODES = 32;

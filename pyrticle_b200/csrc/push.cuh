@@ -90,25 +90,19 @@ static Lagrange<ORDER> make_lagrange(const prt_pusher *P) {
   return L;
 }
 
-// One low-storage RK stage for one live particle in element e:
-//   v = v(p), F = q E(x) + v x (q B(x)), k = a k + dt (v, F), (x, p) += b k,
-// then relocation. Updates xx, pp in place and the residuals kx, kp [3][n]
-// at index i (read and written before the relocation, which keeps them out
-// of its live registers). Returns the new element (PRT_INVALID if the
-// particle left the mesh); *err is set on a locate error.
-template <int ORDER>
-__device__ __forceinline__ uint32_t stage_particle(const DevMesh &M, const Lagrange<ORDER> &L,
-                                                   const Fields6 &F, uint32_t e, double xx[3],
-                                                   double pp[3], double charge, double mass,
-                                                   double *__restrict__ kx,
-                                                   double *__restrict__ kp, long long n,
-                                                   long long i, double a,
-                                                   double b, double dt, double c,
-                                                   unsigned ctr[4], int *err) {
+// The stage after the interpolation: Lorentz force from the fields ef at x,
+// RK update, relocation (shared by the FP64 stage and the mixed-precision
+// stage, whose fields come from the tensor cores).
+__device__ __forceinline__ uint32_t stage_from_fields(const DevMesh &M, uint32_t e,
+                                                      const double ef[6], double xx[3],
+                                                      double pp[3], double charge, double mass,
+                                                      double *__restrict__ kx,
+                                                      double *__restrict__ kp, long long n,
+                                                      long long i, double a, double b,
+                                                      double dt, double c, unsigned ctr[4],
+                                                      int *err) {
   double v[3];
   velocity_exact(pp[0], pp[1], pp[2], mass, c, v[0], v[1], v[2]);
-  double ef[6];
-  interpolate_fields<ORDER>(M, L, F, e, xx[0], xx[1], xx[2], ef);
   double elf[3], qb[3], f[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -129,4 +123,25 @@ __device__ __forceinline__ uint32_t stage_particle(const DevMesh &M, const Lagra
   }
   bool wrapped;
   return relocate(M, xx[0], xx[1], xx[2], pp[0], pp[1], pp[2], e, ctr, err, &wrapped);
+}
+
+// One low-storage RK stage for one live particle in element e:
+//   v = v(p), F = q E(x) + v x (q B(x)), k = a k + dt (v, F), (x, p) += b k,
+// then relocation. Updates xx, pp in place and the residuals kx, kp [3][n]
+// at index i (read and written before the relocation, which keeps them out
+// of its live registers). Returns the new element (PRT_INVALID if the
+// particle left the mesh); *err is set on a locate error.
+template <int ORDER>
+__device__ __forceinline__ uint32_t stage_particle(const DevMesh &M, const Lagrange<ORDER> &L,
+                                                   const Fields6 &F, uint32_t e, double xx[3],
+                                                   double pp[3], double charge, double mass,
+                                                   double *__restrict__ kx,
+                                                   double *__restrict__ kp, long long n,
+                                                   long long i, double a,
+                                                   double b, double dt, double c,
+                                                   unsigned ctr[4], int *err) {
+  double ef[6];
+  interpolate_fields<ORDER>(M, L, F, e, xx[0], xx[1], xx[2], ef);
+  return stage_from_fields(M, e, ef, xx, pp, charge, mass, kx, kp, n, i, a, b, dt, c, ctr,
+                           err);
 }
