@@ -431,7 +431,9 @@ class PicMethod:
         out = None
         for step in range(steps):
             if sort_every and step % sort_every == 0:
-                self.sort_by_element(state)
+                # at a step boundary the residuals are dead (the first stage's
+                # a = 0 overwrites them), so they are not permuted
+                self.sort_by_element(state, residuals=False)
                 kx, kp = state.kx, state.kp
             for a, b in zip(LSRK4_A, LSRK4_B):
                 _lib.check(self.lib.prt_lsrk_stage(
@@ -446,12 +448,15 @@ class PicMethod:
             self.check_status()
         return out
 
-    def sort_by_element(self, state):
+    def sort_by_element(self, state, residuals=True):
+        """Sort the store by containing element; `residuals=False` leaves the
+        LSRK residuals unpermuted (valid only at a step boundary)."""
         kx, kp = state.residuals()
         _lib.check(self.lib.prt_sort_by_element(
             self.workspace, len(state), state.el.data_ptr(), state.x.data_ptr(),
-            state.p.data_ptr(), state.q.data_ptr(), state.m.data_ptr(), kx.data_ptr(),
-            kp.data_ptr(), state.ids.data_ptr(), C.c_void_p(stream_handle())),
+            state.p.data_ptr(), state.q.data_ptr(), state.m.data_ptr(),
+            kx.data_ptr() if residuals else None, kp.data_ptr() if residuals else None,
+            state.ids.data_ptr(), C.c_void_p(stream_handle())),
             "prt_sort_by_element")
         state.derived_quantity_cache.clear()
 

@@ -394,13 +394,17 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+#ifndef PRT_STAGE_MIN_BLOCKS
+#define PRT_STAGE_MIN_BLOCKS 3
+#endif
+
 // One fused stage: velocity, interpolation, Lorentz force, 2N-storage RK
 // update, relocation. Dead particles (PRT_INVALID) are not touched.
 // resident 256-thread CTAs per SM the stage kernel is compiled for: the
 // kernel is latency-bound, so occupancy matters more than registers, up to
 // order 3; order 4 (35 monomials in registers) keeps the larger budget
 template <int ORDER>
-__global__ void __launch_bounds__(256, ORDER >= 4 ? 2 : 3)
+__global__ void __launch_bounds__(256, ORDER >= 4 ? 2 : PRT_STAGE_MIN_BLOCKS)
     lsrk_stage_kernel(DevMesh M, const Lagrange<ORDER> L, Fields6 F, long long n,
                       double *__restrict__ x, double *__restrict__ p,
                       const double *__restrict__ q, const double *__restrict__ mass,
