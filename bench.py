@@ -408,6 +408,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     from pyrticle_b200 import _lib, problems
+    from pyrticle_b200.sharding import allreduce_densities, max_over_ranks
 
     w = problems.make(args.workload, scale=args.scale, seed=1 + rank)
     m, sf = build_method(w, torch)
@@ -427,8 +428,7 @@ def main():
         finally:
             m.depositor.precision = "fp64"
         if world > 1:
-            dist.all_reduce(rho)
-            dist.all_reduce(j)
+            allreduce_densities(rho, j)
         return rho, j
 
     for form in ("fp64", "mixed"):
@@ -460,12 +460,12 @@ def main():
         if world > 1:
             dist.barrier()
         _lib.check(m.lib.prt_workspace_timing(m.workspace, 0))
-        t = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
+        t = e0.elapsed_time(e1)
         if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t = max_over_ranks(t, "cuda")
         kernel = {name: timing_read(m, cat) for cat, name in
                   enumerate(("deposit_gather", "deposit_stage", "lsrk_stage", "sort"))}
-        return float(t.item()), kernel
+        return float(t), kernel
 
     ms64, kernel64 = timed("fp64")
     ms, kernel = timed("mixed")
@@ -519,8 +519,7 @@ def main():
             finally:
                 m.depositor.precision = "fp64"
             if world > 1:
-                dist.all_reduce(rho)
-                dist.all_reduce(j)
+                allreduce_densities(rho, j)
             return rho, j
 
         if world > 1:
@@ -550,10 +549,8 @@ def main():
         f1.record(comp)
         torch.cuda.synchronize()
         ems = f0.elapsed_time(f1)
-        t = torch.tensor([ems], device="cuda", dtype=torch.float64)
         if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
+            ems = max_over_ranks(ems, "cuda")
         e2e = {"value": world * n * args.steps / (ems * 1e-3), "unit": METRIC,
                "h2d_bytes_per_step": int(n * (24 + 24 + 8 + 8 + 4)),
                "d2h_bytes_per_step": int(nn * 4 * 8),
