@@ -418,6 +418,37 @@ int prt_deposit_shape_adjoint(const prt_mesh *mesh, prt_workspace *ws,
                               const double *grad_rho, const double *grad_j,
                               double *lam_x, double *lam_v, void *stream);
 
+/* --------------------------------------------------------- diagnostics --- */
+
+/* Replaces kinetic_energies(ps, c) (diagnostics.hpp:38-58): per particle
+ * (gamma - 1) m c^2, written as p^2 c^2 / (E + m c^2) (the reference's
+ * (p/v - m) c^2 without its 0/0 at p = 0); 0 for removed particles
+ * (elements may be NULL: all live). */
+int prt_kinetic_energies(int64_t n, const double *momenta, const double *masses,
+                         const uint32_t *elements, double vacuum_c, double *out,
+                         void *stream);
+
+/* Sums over the live particles in one fused pass, from which the reference's
+ * beam diagnostics follow (diagnostics.hpp:61-180; pyrticle/log.py:107-325):
+ * total_charge = Q, particle_momentum = P, kinetic energy = KE,
+ * rms_beam_size(d) = sqrt(X2[d] / N), rms_beam_emittance(d, b) from X, X2,
+ * XP, XP2, XXP with x' = p_d / p_b (0 where p_b = 0), rms_energy_spread =
+ * sqrt(KE2 / N - (KE / N - ke_shift)^2), particle_current = QV / length.
+ * KE2 sums (KE - ke_shift)^2: with ke_shift near the mean (a first call's
+ * KE / N) the spread loses no digits to cancellation (the reference's
+ * sqrt(<KE^2> - <KE>^2), tools.hpp:303-322, loses ~12 for a gamma = 2 beam
+ * with 1e-3 momentum spread). `out` is a HOST array; the call synchronises
+ * `stream`. Deterministic (fixed-order sums). */
+enum prt_beam_moment {
+  PRT_BM_COUNT = 0, PRT_BM_CHARGE = 1, PRT_BM_P = 2, PRT_BM_KE = 5, PRT_BM_KE2 = 6,
+  PRT_BM_X = 7, PRT_BM_X2 = 10, PRT_BM_XP = 13, PRT_BM_XP2 = 16, PRT_BM_XXP = 19,
+  PRT_BM_QV = 22, PRT_BEAM_MOMENTS = 25
+};
+int prt_beam_moments(prt_workspace *ws, int64_t n, const double *positions,
+                     const double *momenta, const double *charges, const double *masses,
+                     const uint32_t *elements, double vacuum_c, int32_t beam_axis,
+                     double ke_shift, double out[PRT_BEAM_MOMENTS], void *stream);
+
 /* ---------------------------------------------------------------- misc --- */
 
 /* Sorts the particle store by containing element (stable), permuting every

@@ -38,6 +38,8 @@ TIME_SORT = 3
 TIME_STAGE_ADJOINT = 4
 TIME_DEPOSIT_ADJOINT = 5
 MAX_FIELD_BASIS = 4
+BEAM_MOMENTS = 25
+BM = dict(count=0, charge=1, p=2, ke=5, ke2=6, x=7, x2=10, xp=13, xp2=16, xxp=19, qv=22)
 
 DEPOSIT_PLAIN = 0
 DEPOSIT_NORMALIZED = 1
@@ -163,6 +165,8 @@ SIGNATURES = {
     "prt_fields_to_monomial": (_i32, [_vp, _i32, C.POINTER(_vp), C.POINTER(_vp), _vp]),
     "prt_deposit_shape_adjoint": (_i32, [_vp, _vp, ShapeFunctionDesc, _i64, _vp, _vp, _vp,
                                          _vp, _vp, _vp, _vp, _vp, _vp]),
+    "prt_kinetic_energies": (_i32, [_i64, _vp, _vp, _vp, _d, _vp, _vp]),
+    "prt_beam_moments": (_i32, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _d, _i32, _d, _dp, _vp]),
     "prt_version": (C.c_char_p, []),
 }
 

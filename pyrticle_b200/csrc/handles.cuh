@@ -21,6 +21,7 @@ enum {
   PRT_WS_DEP_VALUES,
   PRT_WS_ADJ_POSITIONS,
   PRT_WS_ADJ_PARTIALS,
+  PRT_WS_DIAGNOSTICS,
   PRT_WS_SLOTS
 };
 
