@@ -251,26 +251,51 @@ def cpu_baseline(w, target_seconds, threads=0, steps=1, seed=7):
     rng = np.random.default_rng(seed)
     threads = threads or O.max_threads()
 
-    def run(n):
+    def sample(n):
         idx = np.sort(rng.choice(w.particle_count, size=n, replace=False))
-        x, p = w.positions[idx], w.momenta[idx]
-        el = O.find_containing_elements(om, x, linear=False)
+        x = w.positions[idx]
+        return idx, x, O.find_containing_elements(om, x, linear=False)
+
+    def run(n):
+        idx, x, el = sample(n)
         t0 = time.perf_counter()
-        r = O.pic_steps_parallel(pu, om, x, p, w.charges[idx], w.masses[idx], el,
+        r = O.pic_steps_parallel(pu, om, x, w.momenta[idx], w.charges[idx], w.masses[idx], el,
                                  list(w.fields), LSRK4_A, LSRK4_B, w.dt, c, steps, sf,
                                  threads=threads)
         dt = time.perf_counter() - t0
         assert r["rc"] == 0
         return dt
 
-    n = 200
-    dt = run(n)
-    per = dt / n
-    n = int(max(200, min(w.particle_count, target_seconds / max(per, 1e-9))))
-    dt = run(n)
-    return {"value": n * steps / dt, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": f"{n} random particles of the workload x {steps} step(s) on the full "
-                      f"mesh/fields, oracle OpenMP build ({dt:.1f} s)"}
+    # two sizes: the per-particle (marginal) cost excludes the fixed cost of
+    # a deposition over the full node set, which a full-size run amortises
+    n1 = 2000
+    t1 = run(n1)
+    n2 = int(max(4 * n1, min(w.particle_count, 2 * n1 * target_seconds / max(t1, 1e-9))))
+    t2 = run(n2)
+    marginal = (t2 - t1) / (n2 - n1)
+    out = {"value": steps / marginal if marginal > 0 else n2 * steps / t2, "unit": METRIC,
+           "cores": threads, "kind": "port",
+           "value_including_fixed_cost": n2 * steps / t2,
+           "sample": f"{n1} and {n2} random particles of the workload x {steps} step(s) on the "
+                     f"full mesh/fields, oracle OpenMP build ({t1:.1f} s, {t2:.1f} s); value = "
+                     f"1 / per-particle cost from the two sizes"}
+    # one core: the reference's serial algorithms (oracle serial build)
+    pu1 = O.OraclePusher(ex, refelement.monomial_vandermonde(refelement.unit_nodes(w.order), ex))
+    ts = []
+    for n in (n1 // 4, n1):
+        idx, x, el = sample(n)
+        t0 = time.perf_counter()
+        r = O.lsrk_steps(pu1, om, x, w.momenta[idx], w.charges[idx], w.masses[idx], el,
+                         list(w.fields), LSRK4_A, LSRK4_B, w.dt, c, steps)
+        O.deposit_shape(om, 0, sf, r["x"], r["q"], O.velocities(r["p"], r["m"], c), r["el"])
+        ts.append((n, time.perf_counter() - t0))
+    (na, ta), (nb, tb) = ts
+    m1 = (tb - ta) / (nb - na)
+    out["one_core"] = {"value": steps / m1 if m1 > 0 else nb * steps / tb, "unit": METRIC,
+                       "cores": 1, "kind": "port",
+                       "sample": f"{na} and {nb} particles x {steps} step(s), oracle serial "
+                                 f"build ({ta:.1f} s, {tb:.1f} s)"}
+    return out
 
 
 def run_reference(args):

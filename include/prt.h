@@ -49,7 +49,10 @@ enum prt_status {
 enum prt_warning {
   PRT_WARN_NONE = 0,
   /* "deposited particle mass is zero" (dep_normshape.hpp:179-185) */
-  PRT_WARN_ZERO_MASS = 1
+  PRT_WARN_ZERO_MASS = 1,
+  /* "average pusher: particle %d had zero reconstructed charge"
+   * (push_average.hpp:161-166) */
+  PRT_WARN_ZERO_AVERAGE = 2
 };
 
 /* ---------------------------------------------------------------- mesh --- */
@@ -417,6 +420,32 @@ int prt_deposit_shape_adjoint(const prt_mesh *mesh, prt_workspace *ws,
                               const double *velocities, const uint32_t *elements,
                               const double *grad_rho, const double *grad_j,
                               double *lam_x, double *lam_v, void *stream);
+
+/* ---------------------------------------------------- averaging pusher --- */
+
+/* Replaces AveragingPusher3d3v(mesh, mass_matrix).forces(ex, ey, ez, bx, by,
+ * bz, ps, pusher_state, depositor, depositor_state, velocities, vis_listener)
+ * (push_average.hpp:330-420, wrap_pusher.cpp): forces[3][n] = q <E> +
+ * v x (q <B>), <F> the average of the nodal field over the nodes within the
+ * shape radius weighted by |J_e| w_i S(x_i - x_p) (integral_weights: HOST
+ * [Np], w = M 1). Zero force and PRT_WARN_ZERO_AVERAGE for a particle with
+ * no weight. vis (NULL or [14][n]): pt_e (3), pt_b (3), pt_e_stddev,
+ * pt_b_stddev, el_force (3), mag_force (3). scales (NULL or [n]): the
+ * normalisation q / (reconstructed charge) of each particle (the pusher
+ * state's statistics). */
+int prt_average_forces(const prt_mesh *mesh, prt_workspace *ws, prt_shape_function shape,
+                       const double *integral_weights, int64_t n, const double *positions,
+                       const double *charges, const double *velocities,
+                       const uint32_t *elements, const double *const fields[6],
+                       double *forces, double *vis, double *scales, void *stream);
+
+/* One low-storage RK stage from given forces (a pusher whose forces come
+ * from a separate pass): k = a k + dt (v(p), F), (x, p) += b k, relocation,
+ * as prt_lsrk_stage after its force. */
+int prt_lsrk_update(const prt_mesh *mesh, prt_workspace *ws, int64_t n, double *positions,
+                    double *momenta, const double *masses, uint32_t *elements, double *kx,
+                    double *kp, const double *forces, double rk_a, double rk_b, double dt,
+                    double vacuum_c, void *stream);
 
 /* --------------------------------------------------------- diagnostics --- */
 

@@ -28,6 +28,7 @@ ERRORS = {
     -7: "a kernel's bounded wait on its tensor-core work timed out",
 }
 PRT_WARN_ZERO_MASS = 1
+PRT_WARN_ZERO_AVERAGE = 2
 PRT_ERR_CAPACITY = -6
 NOALLOC_SCRATCH_BYTES = 64 << 20
 
@@ -165,6 +166,10 @@ SIGNATURES = {
     "prt_fields_to_monomial": (_i32, [_vp, _i32, C.POINTER(_vp), C.POINTER(_vp), _vp]),
     "prt_deposit_shape_adjoint": (_i32, [_vp, _vp, ShapeFunctionDesc, _i64, _vp, _vp, _vp,
                                          _vp, _vp, _vp, _vp, _vp, _vp]),
+    "prt_average_forces": (_i32, [_vp, _vp, ShapeFunctionDesc, _dp, _i64, _vp, _vp, _vp, _vp,
+                                  C.POINTER(_vp), _vp, _vp, _vp, _vp]),
+    "prt_lsrk_update": (_i32, [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _d,
+                               _d, _vp]),
     "prt_kinetic_energies": (_i32, [_i64, _vp, _vp, _vp, _d, _vp, _vp]),
     "prt_beam_moments": (_i32, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _d, _i32, _d, _dp, _vp]),
     "prt_version": (C.c_char_p, []),

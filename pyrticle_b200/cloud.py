@@ -255,6 +255,10 @@ class PicMethod:
             from .tools import warning_forwarder
             warning_forwarder.note_warning(
                 "deposited particle mass is zero (particle %d)" % widx.value)
+        elif warn.value == _lib.PRT_WARN_ZERO_AVERAGE:
+            from .tools import warning_forwarder
+            warning_forwarder.note_warning(
+                "average pusher: particle %d had zero reconstructed charge" % widx.value)
         if err.value:
             raise RuntimeError("%s (particle %d)" % (_lib.ERRORS.get(err.value, err.value),
                                                      eidx.value))
@@ -436,11 +440,7 @@ class PicMethod:
                 self.sort_by_element(state, residuals=False)
                 kx, kp = state.kx, state.kp
             for a, b in zip(LSRK4_A, LSRK4_B):
-                _lib.check(self.lib.prt_lsrk_stage(
-                    self.pusher.handle, self.workspace, len(state), state.x.data_ptr(),
-                    state.p.data_ptr(), state.q.data_ptr(), state.m.data_ptr(),
-                    state.el.data_ptr(), kx.data_ptr(), kp.data_ptr(), fptrs, a, b, dt, c,
-                    precision, s), "prt_lsrk_stage")
+                self.pusher.lsrk_stage(state, fptrs, kx, kp, a, b, dt, c, precision)
             state.derived_quantity_cache.clear()
             if deposit:
                 out = self.deposit_densities_device(state)

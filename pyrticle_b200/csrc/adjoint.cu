@@ -27,7 +27,7 @@
 
 #include <cmath>
 
-#include "binning.cuh"
+#include "gather.cuh"
 #include "push.cuh"
 
 namespace {
@@ -357,32 +357,14 @@ __global__ void contract_kernel(long long npos, long long nn,
   for (int d = 0; d < 4; ++d) G[d * npos + u] = s[d];
 }
 
-struct CentreBinsDev {
-  double origin[3], inv_w[3];
-  int dims[3];
-  double max_radius;
-  const uint32_t *__restrict__ starts;
-  const double *__restrict__ spheres;
-  const uint32_t *__restrict__ ranges;
-};
-
 constexpr int DEP_ADJ_BLOCK = 128;
 
 // Adjoint of the plain shape deposition. With weight w = q N and
 // S = (a - r^2/a)^alpha:
 //   dL/dx_p = w sum_u (G0_u + G_u . v_p) dS/dx_p,
-//   dL/dv_p = w sum_u G_u S,   dS/dx_p = alpha (a - r^2/a)^(alpha-1) (2/a) (x_u - x_p).
-// Lane = particle; a warp takes 32 consecutive particles (element-sorted
-// particles are spatially close) and walks the position groups whose centre
-// bin lies within a + (largest group radius) of the warp's bounding box: the
-// lanes test 32 candidate groups at a time against the box (ballot), then
-// for each surviving group that reaches some lane's particle the warp stages
-// the group's positions and node adjoints in shared memory and every lane
-// evaluates its particle against all of them, branch-free (zero weight
-// beyond the radius). Each particle's sums run in a fixed order: no atomics,
-// deterministic. Periodic axes: the warp also walks the images of its box
-// shifted by a period where the box comes within the radius of the
-// periodicity interval's end.
+//   dL/dv_p = w sum_u G_u S,   dS/dx_p = alpha (a - r^2/a)^(alpha-1) (2/a) (x_u - x_p),
+// gathered per particle (lane) over the positions within the radius
+// (warp_gather_positions, gather.cuh).
 template <bool ALPHA2>
 __global__ void __launch_bounds__(DEP_ADJ_BLOCK, 4)
     deposit_adjoint_kernel(DevMesh M, CentreBinsDev CB, const double *__restrict__ pos,
@@ -391,8 +373,8 @@ __global__ void __launch_bounds__(DEP_ADJ_BLOCK, 4)
                            const double *__restrict__ x, const double *__restrict__ q,
                            const double *__restrict__ v, const uint32_t *__restrict__ el,
                            double *__restrict__ lx, double *__restrict__ lv) {
-  __shared__ double2 stage[DEP_ADJ_BLOCK / 32][32][4];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ GatherStage<4> stage[DEP_ADJ_BLOCK / 32];
+  const int warp = threadIdx.x >> 5;
   const long long i = blockIdx.x * (long long)DEP_ADJ_BLOCK + threadIdx.x;
   const bool live = i < n && (!el || el[i] != PRT_INVALID);
   double p[3] = {0, 0, 0}, vv[3] = {0, 0, 0};
@@ -403,112 +385,29 @@ __global__ void __launch_bounds__(DEP_ADJ_BLOCK, 4)
       if (v) vv[d] = v[d * n + i];
     }
   }
-  if (!__any_sync(0xffffffffu, live)) return;  // warp-uniform
-  double blo[3], bhi[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    blo[d] = live ? p[d] : INFINITY;
-    bhi[d] = live ? p[d] : -INFINITY;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      blo[d] = fmin(blo[d], __shfl_xor_sync(0xffffffffu, blo[d], o));
-      bhi[d] = fmax(bhi[d], __shfl_xor_sync(0xffffffffu, bhi[d], o));
-    }
-  }
-  int lo_img[3], hi_img[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    lo_img[d] = hi_img[d] = 0;
-    if (M.pmin[d] != M.pmax[d]) {
-      if (blo[d] - S.radius < M.pmin[d]) hi_img[d] = 1;
-      if (bhi[d] + S.radius > M.pmax[d]) lo_img[d] = -1;
-    }
-  }
-  const double reach = S.radius + CB.max_radius;
   double ax0 = 0, ax1 = 0, ax2 = 0, as1 = 0, as2 = 0, as3 = 0;
-  for (int iz = lo_img[2]; iz <= hi_img[2]; ++iz)
-    for (int iy = lo_img[1]; iy <= hi_img[1]; ++iy)
-      for (int ix = lo_img[0]; ix <= hi_img[0]; ++ix) {
-        const double sh[3] = {ix * (M.pmax[0] - M.pmin[0]), iy * (M.pmax[1] - M.pmin[1]),
-                              iz * (M.pmax[2] - M.pmin[2])};
-        const double c0 = p[0] + sh[0], c1 = p[1] + sh[1], c2 = p[2] + sh[2];
-        double qlo[3], qhi[3];
-        int b0[3], b1[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          qlo[d] = blo[d] + sh[d];
-          qhi[d] = bhi[d] + sh[d];
-          const double l = floor((qlo[d] - reach - CB.origin[d]) * CB.inv_w[d]);
-          const double h = floor((qhi[d] + reach - CB.origin[d]) * CB.inv_w[d]);
-          b0[d] = (int)fmax(0.0, fmin(l, CB.dims[d] - 1.0));
-          b1[d] = (int)fmax(0.0, fmin(h, CB.dims[d] - 1.0));
+  warp_gather_positions<4>(
+      M, CB, pos, npos, G, S.radius, live, p, stage[warp],
+      [&](double f0, double f1, double f2, double r2, const double *g) {
+        const double rt = fmax(fma(-r2, S.inv_radius, S.radius), 0.0);
+        double sv, ds;
+        if (ALPHA2) {
+          sv = rt * rt;
+          ds = rt * (4.0 * S.inv_radius);
+        } else {
+          const double pm = rt > 0 ? pow(rt, S.alpha - 1.0) : 0.0;
+          sv = pm * rt;
+          ds = S.alpha * pm * (2.0 * S.inv_radius);
         }
-        for (int bz = b0[2]; bz <= b1[2]; ++bz)
-          for (int by = b0[1]; by <= b1[1]; ++by) {
-            const long long row = (long long)CB.dims[0] * (by + (long long)CB.dims[1] * bz);
-            const uint32_t k0 = CB.starts[row + b0[0]], k1 = CB.starts[row + b1[0] + 1];
-            for (uint32_t kb = k0; kb < k1; kb += 32) {
-              const uint32_t k = kb + lane;
-              bool cand = false;
-              if (k < k1) {
-                const double *sp = CB.spheres + 4 * (size_t)k;
-                double d2 = 0;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                  const double e = fmax(0.0, fmax(qlo[d] - sp[d], sp[d] - qhi[d]));
-                  d2 = fma(e, e, d2);
-                }
-                const double lim = S.radius + sp[3];
-                cand = d2 <= lim * lim;
-              }
-              unsigned mask = __ballot_sync(0xffffffffu, cand);
-              while (mask) {
-                const int j = __ffs(mask) - 1;
-                mask &= mask - 1;
-                const uint32_t kk = kb + j;
-                const double *sp = CB.spheres + 4 * (size_t)kk;
-                const double e0 = sp[0] - c0, e1 = sp[1] - c1, e2 = sp[2] - c2;
-                const double lim = S.radius + sp[3];
-                const bool hit = live && e0 * e0 + e1 * e1 + e2 * e2 <= lim * lim;
-                if (!__any_sync(0xffffffffu, hit)) continue;
-                const uint32_t u0 = CB.ranges[2 * (size_t)kk], cnt = CB.ranges[2 * (size_t)kk + 1];
-                if ((uint32_t)lane < cnt) {
-                  const long long u = u0 + lane;
-                  stage[warp][lane][0] = make_double2(pos[3 * u], pos[3 * u + 1]);
-                  stage[warp][lane][1] = make_double2(pos[3 * u + 2], G[u]);
-                  stage[warp][lane][2] = make_double2(G[npos + u], G[2 * npos + u]);
-                  stage[warp][lane][3] = make_double2(G[3 * npos + u], 0.0);
-                }
-                __syncwarp();
-                for (uint32_t t = 0; t < cnt; ++t) {
-                  const double2 s0 = stage[warp][t][0], s1 = stage[warp][t][1],
-                                s2 = stage[warp][t][2], s3 = stage[warp][t][3];
-                  const double f0 = s0.x - c0, f1 = s0.y - c1, f2 = s1.x - c2;
-                  const double r2 = fma(f0, f0, fma(f1, f1, f2 * f2));
-                  const double rt = fmax(fma(-r2, S.inv_radius, S.radius), 0.0);
-                  double sv, ds;
-                  if (ALPHA2) {
-                    sv = rt * rt;
-                    ds = rt * (4.0 * S.inv_radius);
-                  } else {
-                    const double pm = rt > 0 ? pow(rt, S.alpha - 1.0) : 0.0;
-                    sv = pm * rt;
-                    ds = S.alpha * pm * (2.0 * S.inv_radius);
-                  }
-                  const double h = fma(s2.y, vv[1], fma(s2.x, vv[0], fma(s3.x, vv[2], s1.y)));
-                  const double hd = h * ds;
-                  ax0 = fma(hd, f0, ax0);
-                  ax1 = fma(hd, f1, ax1);
-                  ax2 = fma(hd, f2, ax2);
-                  as1 = fma(s2.x, sv, as1);
-                  as2 = fma(s2.y, sv, as2);
-                  as3 = fma(s3.x, sv, as3);
-                }
-                __syncwarp();
-              }
-            }
-          }
-      }
+        const double h = fma(g[2], vv[1], fma(g[1], vv[0], fma(g[3], vv[2], g[0])));
+        const double hd = h * ds;
+        ax0 = fma(hd, f0, ax0);
+        ax1 = fma(hd, f1, ax1);
+        ax2 = fma(hd, f2, ax2);
+        as1 = fma(g[1], sv, as1);
+        as2 = fma(g[2], sv, as2);
+        as3 = fma(g[3], sv, as3);
+      });
   if (live) {
     const double w = q[i] * normalizer;
     lx[i] += w * ax0;
@@ -709,17 +608,7 @@ extern "C" int prt_deposit_shape_adjoint(const prt_mesh *mesh, prt_workspace *ws
   S.inv_radius = 1.0 / shape.radius;
   S.alpha = shape.alpha;
   for (int d = 0; d < 3; ++d) S.reach[d] = shape.radius;
-  const auto &H = PS.centre_bins;
-  CentreBinsDev CB;
-  for (int d = 0; d < 3; ++d) {
-    CB.origin[d] = H.origin[d];
-    CB.inv_w[d] = H.inv_w[d];
-    CB.dims[d] = H.dims[d];
-  }
-  CB.max_radius = H.max_radius;
-  CB.starts = H.starts;
-  CB.spheres = H.spheres;
-  CB.ranges = H.ranges;
+  const CentreBinsDev CB = centre_bins_dev(PS);
   const double *vv = grad_j ? v : nullptr;
   double *lvv = grad_j ? lam_v : nullptr;
   const unsigned blocks = (unsigned)((n + DEP_ADJ_BLOCK - 1) / DEP_ADJ_BLOCK);

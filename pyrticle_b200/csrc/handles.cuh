@@ -22,6 +22,7 @@ enum {
   PRT_WS_ADJ_POSITIONS,
   PRT_WS_ADJ_PARTIALS,
   PRT_WS_DIAGNOSTICS,
+  PRT_WS_AVERAGE,
   PRT_WS_SLOTS
 };
 

@@ -90,28 +90,17 @@ static Lagrange<ORDER> make_lagrange(const prt_pusher *P) {
   return L;
 }
 
-// The stage after the interpolation: Lorentz force from the fields ef at x,
-// RK update, relocation (shared by the FP64 stage and the mixed-precision
-// stage, whose fields come from the tensor cores).
-__device__ __forceinline__ uint32_t stage_from_fields(const DevMesh &M, uint32_t e,
-                                                      const double ef[6], double xx[3],
-                                                      double pp[3], double charge, double mass,
-                                                      double *__restrict__ kx,
-                                                      double *__restrict__ kp, long long n,
-                                                      long long i, double a, double b,
-                                                      double dt, double c, unsigned ctr[4],
-                                                      int *err) {
-  double v[3];
-  velocity_exact(pp[0], pp[1], pp[2], mass, c, v[0], v[1], v[2]);
-  double elf[3], qb[3], f[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    elf[d] = __dmul_rn(charge, ef[d]);
-    qb[d] = __dmul_rn(charge, ef[3 + d]);
-  }
-  f[0] = __dadd_rn(elf[0], __dsub_rn(__dmul_rn(v[1], qb[2]), __dmul_rn(v[2], qb[1])));
-  f[1] = __dadd_rn(elf[1], __dsub_rn(__dmul_rn(v[2], qb[0]), __dmul_rn(v[0], qb[2])));
-  f[2] = __dadd_rn(elf[2], __dsub_rn(__dmul_rn(v[0], qb[1]), __dmul_rn(v[1], qb[0])));
+// RK update and relocation from a force f at (x, p): k = a k + dt (v(p), f),
+// (x, p) += b k (residuals kx, kp [3][n] at index i, read and written before
+// the relocation), then the new containing element (PRT_INVALID if the
+// particle left the mesh; *err on a locate error).
+__device__ __forceinline__ uint32_t update_particle(const DevMesh &M, uint32_t e,
+                                                    const double f[3], const double v[3],
+                                                    double xx[3], double pp[3],
+                                                    double *__restrict__ kx,
+                                                    double *__restrict__ kp, long long n,
+                                                    long long i, double a, double b,
+                                                    double dt, unsigned ctr[4], int *err) {
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const double kxd = __dadd_rn(__dmul_rn(a, kx[d * n + i]), __dmul_rn(dt, v[d]));
@@ -123,6 +112,38 @@ __device__ __forceinline__ uint32_t stage_from_fields(const DevMesh &M, uint32_t
   }
   bool wrapped;
   return relocate(M, xx[0], xx[1], xx[2], pp[0], pp[1], pp[2], e, ctr, err, &wrapped);
+}
+
+// Lorentz force F = q E + v x (q B) in the reference's operation order
+// (push_monomial.hpp:219-325).
+__device__ __forceinline__ void lorentz_force(double charge, const double ef[6],
+                                              const double v[3], double f[3]) {
+  double elf[3], qb[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    elf[d] = __dmul_rn(charge, ef[d]);
+    qb[d] = __dmul_rn(charge, ef[3 + d]);
+  }
+  f[0] = __dadd_rn(elf[0], __dsub_rn(__dmul_rn(v[1], qb[2]), __dmul_rn(v[2], qb[1])));
+  f[1] = __dadd_rn(elf[1], __dsub_rn(__dmul_rn(v[2], qb[0]), __dmul_rn(v[0], qb[2])));
+  f[2] = __dadd_rn(elf[2], __dsub_rn(__dmul_rn(v[0], qb[1]), __dmul_rn(v[1], qb[0])));
+}
+
+// The stage after the interpolation: Lorentz force from the fields ef at x,
+// RK update, relocation (shared by the FP64 stage and the mixed-precision
+// stage, whose fields come from the tensor cores).
+__device__ __forceinline__ uint32_t stage_from_fields(const DevMesh &M, uint32_t e,
+                                                      const double ef[6], double xx[3],
+                                                      double pp[3], double charge, double mass,
+                                                      double *__restrict__ kx,
+                                                      double *__restrict__ kp, long long n,
+                                                      long long i, double a, double b,
+                                                      double dt, double c, unsigned ctr[4],
+                                                      int *err) {
+  double v[3], f[3];
+  velocity_exact(pp[0], pp[1], pp[2], mass, c, v[0], v[1], v[2]);
+  lorentz_force(charge, ef, v, f);
+  return update_particle(M, e, f, v, xx, pp, kx, kp, n, i, a, b, dt, ctr, err);
 }
 
 // One low-storage RK stage for one live particle in element e:
