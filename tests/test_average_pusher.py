@@ -76,7 +76,8 @@ def test_average_pusher_static_fields():
         mesh = SF.periodic_cylinder_box()
         m = PicMethod(Discretization(mesh, 1), U, ShapeFunctionDepositor(),
                       AverageParticlePusher(), 3, 3)
-        m.depositor.set_shape_function(None, PolynomialShapeFunction(0.3, 3, 2))
+        # the order-1 nodes are 0.5 apart: a radius of 0.6 always reaches some
+        m.depositor.set_shape_function(None, PolynomialShapeFunction(0.6, 3, 2))
         nodes = m.discretization.nodes
         fields = torch.as_tensor(SF.uniform_fields(nodes, setup_.e(), setup_.b()), device="cuda")
         x0 = setup_.positions(0)
