@@ -330,6 +330,12 @@ typedef struct prt_grid_desc {
   int64_t avg_group_count;
   const uint32_t *avg_group_starts; /* [avg_group_count+1] */
   const uint32_t *avg_group_nodes;
+  /* Jiggly bricks (JigglyBrick, grid.hpp:345-449): NULL for regular
+   * cell-centred points, else [brick_count][3][3], per brick its three point
+   * origins; point idx of brick b is point_origins[b][(i + j + k) % 3] +
+   * idx * stepwidths. Every offset must stay within half a cell. Shape
+   * weights only (PRT_GRID_TRILINEAR is rejected). */
+  const double *point_origins;
 } prt_grid_desc;
 
 int prt_grid_create(const prt_mesh *mesh, const prt_grid_desc *desc,

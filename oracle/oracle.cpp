@@ -542,9 +542,14 @@ struct Brick {
   int dims[3];
   int64_t strides[3];
   int64_t start;
+  // jiggly_brick (grid.hpp:345-449): three point origins, chosen per point
+  // by (i + j + k) % 3
+  bool jiggly;
+  double po[3][3];
 };
 
-Brick make_brick(const prt_brick &b) {
+// `po`: the brick's three point origins ([3][3]) for a jiggly brick, or NULL
+Brick make_brick(const prt_brick &b, const double *po = nullptr) {
   Brick r;
   for (int d = 0; d < 3; ++d) {
     r.origin[d] = b.origin[d];
@@ -556,7 +561,21 @@ Brick make_brick(const prt_brick &b) {
   r.strides[1] = r.dims[0];
   r.strides[2] = (int64_t)r.dims[0] * r.dims[1];
   r.start = b.start_index;
+  r.jiggly = po != nullptr;
+  for (int i = 0; i < 3; ++i)
+    for (int d = 0; d < 3; ++d) r.po[i][d] = po ? po[3 * i + d] : 0.0;
   return r;
+}
+
+// jiggly_brick::point (grid.hpp:386-396): point_origins[(i+j+k) % 3] + idx h.
+// The reference's jiggly iterator (grid.hpp:398-440) instead advances along x
+// by the offset of the origin AFTER the next one (it bumps the origin index
+// before choosing the offset), so its points along a row depend on where the
+// row starts; this restatement, like the device path, uses point(idx).
+void jiggly_point(const Brick &b, int i, int j, int k, double pt[3]) {
+  const int oi = (i + j + k) % 3;
+  const int idx[3] = {i, j, k};
+  for (int d = 0; d < 3; ++d) pt[d] = b.po[oi][d] + idx[d] * b.h[d];
 }
 
 // grid_depositor::deposit_particle_on_one_brick (dep_grid.hpp:220-264) with
@@ -591,6 +610,7 @@ bool deposit_on_brick(const Brick &brk, const Shape &sf, const double *center,
                       brk.oph[2] + k * brk.h[2]};
       int64_t idx = brk.start + lo[0] + brk.strides[1] * j + brk.strides[2] * k;
       for (int i = lo[0]; i < hi[0]; ++i) {
+        if (brk.jiggly) jiggly_point(brk, i, j, k, pt);
         double d[3] = {center[0] - pt[0], center[1] - pt[1], center[2] - pt[2]};
         add(idx, charge * sf(d));
         pt[0] += brk.h[0];
@@ -598,6 +618,66 @@ bool deposit_on_brick(const Brick &brk, const Shape &sf, const double *center,
       }
     }
   return true;
+}
+
+// deposit_densities_on_grid_target + deposit_periodic_copies +
+// deposit_single_particle_with/without_cache (dep_grid_base.hpp:210-382) for
+// one particle at x: the particle box [x - a, x + a], then recursively its
+// periodic copies, one per set of axes crossed (at most one image per axis:
+// the lower end first). on_brick(brick, center, box_lo, box_hi, complete*)
+// deposits on one brick and returns whether the box met it. `cache` (or
+// NULL: every brick, no cache) is this particle's brick cache.
+template <class OnBrick>
+void deposit_periodic_copies(const prt_mesh_desc &m, const std::vector<Brick> &B,
+                             double radius, const double *x, uint32_t *cache,
+                             OnBrick &&on_brick) {
+  std::vector<unsigned> pset;
+  struct Frame {
+    double c[3], lo[3], hi[3];
+    unsigned abf;
+  };
+  auto go = [&](auto &&self, const Frame &f) -> void {
+    if (f.abf == 0 && cache) {
+      uint32_t &bn = *cache;
+      bool complete;
+      const bool hit_cached = on_brick(B[bn], f.c, f.lo, f.hi, &complete);
+      if (!complete)
+        for (size_t bi = 0; bi < B.size(); ++bi) {
+          if (bi == bn) continue;
+          if (on_brick(B[bi], f.c, f.lo, f.hi, nullptr) && !hit_cached) bn = (uint32_t)bi;
+        }
+    } else {
+      for (const Brick &b : B) on_brick(b, f.c, f.lo, f.hi, nullptr);
+    }
+    pset.push_back(f.abf);
+    for (int axis = 0; axis < 3; ++axis) {
+      const double mn = m.periodicity_min[axis], mx = m.periodicity_max[axis];
+      if (mn == mx) continue;
+      const unsigned abf2 = f.abf | (1u << axis);
+      if (std::find(pset.begin(), pset.end(), abf2) != pset.end()) continue;
+      double off;
+      if (f.lo[axis] < mn)
+        off = mx - mn;
+      else if (f.hi[axis] > mx)
+        off = -(mx - mn);
+      else
+        continue;
+      Frame g = f;
+      g.c[axis] += off;
+      g.lo[axis] += off;
+      g.hi[axis] += off;
+      g.abf = abf2;
+      self(self, g);
+    }
+  };
+  Frame f0;
+  for (int d = 0; d < 3; ++d) {
+    f0.c[d] = x[d];
+    f0.lo[d] = x[d] - radius;
+    f0.hi[d] = x[d] + radius;
+  }
+  f0.abf = 0;
+  go(go, f0);
 }
 
 }  // namespace
@@ -757,14 +837,15 @@ int orc_walk_elements(const prt_mesh_desc *m, const double *pos, uint32_t start,
 // per-particle brick cache and periodic copies. weights: PRT_GRID_SHAPE or
 // PRT_GRID_TRILINEAR. grid_rho [G], grid_j [G][3] are zeroed first.
 int orc_deposit_grid(const prt_mesh_desc *m, int nbricks, const prt_brick *bricks,
-                     int weights, prt_shape_function shape, int64_t n,
-                     const double *x, const double *q, const double *v,
+                     const double *point_origins, int weights, prt_shape_function shape,
+                     int64_t n, const double *x, const double *q, const double *v,
                      int64_t gnc, double *grid_rho, double *grid_j,
                      uint32_t *brick_cache) {
   if (grid_rho) std::memset(grid_rho, 0, gnc * sizeof(double));
   if (grid_j) std::memset(grid_j, 0, 3 * gnc * sizeof(double));
   std::vector<Brick> B;
-  for (int i = 0; i < nbricks; ++i) B.push_back(make_brick(bricks[i]));
+  for (int i = 0; i < nbricks; ++i)
+    B.push_back(make_brick(bricks[i], point_origins ? point_origins + 9 * i : nullptr));
   Shape sf = make_shape(shape);
   for (int64_t pn = 0; pn < n; ++pn) {
     const double *c0 = x + 3 * pn;
@@ -810,58 +891,78 @@ int orc_deposit_grid(const prt_mesh_desc *m, int nbricks, const prt_brick *brick
       }
       continue;
     }
-    // periodic copies (dep_grid_base.hpp:285-347), recursion over axis sets
-    std::vector<unsigned> pset;
-    struct Rec {
-      static void go(const prt_mesh_desc *m, std::vector<Brick> &B, const Shape &sf,
-                     int64_t pn, const double *q, const double *center,
-                     const double *plo, const double *phi, unsigned abf,
-                     std::vector<unsigned> &pset, uint32_t *cache,
-                     decltype(add) &add) {
-        if (abf == 0 && cache) {
-          uint32_t &bn = cache[pn];
-          const Brick &last = B[bn];
-          bool complete;
-          bool hit_cached = deposit_on_brick(last, sf, center, plo, phi, q[pn], &complete, add);
-          if (!complete)
-            for (size_t bi = 0; bi < B.size(); ++bi) {
-              if (bi == bn) continue;
-              if (deposit_on_brick(B[bi], sf, center, plo, phi, q[pn], nullptr, add) &&
-                  !hit_cached)
-                bn = (uint32_t)bi;
-            }
-        } else {
-          for (const Brick &b : B)
-            deposit_on_brick(b, sf, center, plo, phi, q[pn], nullptr, add);
-        }
-        pset.push_back(abf);
-        for (int axis = 0; axis < 3; ++axis) {
-          double mn = m->periodicity_min[axis], mx = m->periodicity_max[axis];
-          if (mn == mx) continue;
-          unsigned abf2 = abf | (1u << axis);
-          if (std::find(pset.begin(), pset.end(), abf2) != pset.end()) continue;
-          double off = 0;
-          if (plo[axis] < mn)
-            off = mx - mn;
-          else if (phi[axis] > mx)
-            off = -(mx - mn);
-          else
-            continue;
-          double c2[3] = {center[0], center[1], center[2]};
-          double l2[3] = {plo[0], plo[1], plo[2]}, h2[3] = {phi[0], phi[1], phi[2]};
-          c2[axis] += off;
-          l2[axis] += off;
-          h2[axis] += off;
-          go(m, B, sf, pn, q, c2, l2, h2, abf2, pset, cache, add);
-        }
-      }
+    auto on_brick = [&](const Brick &b, const double *center, const double *plo,
+                        const double *phi, bool *complete) {
+      return deposit_on_brick(b, sf, center, plo, phi, q[pn], complete, add);
     };
-    double plo[3], phi[3];
-    for (int d = 0; d < 3; ++d) {
-      plo[d] = c0[d] - sf.radius;
-      phi[d] = c0[d] + sf.radius;
-    }
-    Rec::go(m, B, sf, pn, q, c0, plo, phi, 0, pset, brick_cache, add);
+    deposit_periodic_copies(*m, B, sf.radius, c0, brick_cache ? brick_cache + pn : nullptr,
+                            on_brick);
+  }
+  return 0;
+}
+
+// grid_find_depositor (dep_grid_find.hpp:33-184; node lists from
+// grid_find.py:55-104): every particle (and each of its periodic copies,
+// with the brick cache, dep_grid_base.hpp:175-382) walks the cells of
+// index_range(brick box & particle box) of each brick and adds
+// q S(center - node) to every mesh node in the cell's node list.
+// cell_starts [G+1] / cell_nodes: the node numbers per global grid index.
+// nodes [Nn][3]; rho [Nn] and j [Nn][3] are zeroed first.
+int orc_deposit_grid_find(const prt_mesh_desc *m, int nbricks, const prt_brick *bricks,
+                          const uint32_t *cell_starts, const uint32_t *cell_nodes,
+                          const double *nodes, int64_t nn, prt_shape_function shape,
+                          int64_t n, const double *x, const double *q, const double *v,
+                          double *rho, double *j, uint32_t *brick_cache) {
+  if (rho) std::memset(rho, 0, nn * sizeof(double));
+  if (j) std::memset(j, 0, 3 * nn * sizeof(double));
+  std::vector<Brick> B;
+  for (int i = 0; i < nbricks; ++i) B.push_back(make_brick(bricks[i]));
+  Shape sf = make_shape(shape);
+  for (int64_t pn = 0; pn < n; ++pn) {
+    double sfac[3] = {0, 0, 0};
+    if (j)
+      for (int a = 0; a < 3; ++a) sfac[a] = v[3 * pn + a];
+    // deposit_particle_on_one_brick (dep_grid_find.hpp:73-112)
+    auto on_brick = [&](const Brick &brk, const double *center, const double *plo,
+                        const double *phi, bool *complete) {
+      double ilo[3], ihi[3];
+      for (int d = 0; d < 3; ++d) {
+        ilo[d] = std::max(brk.origin[d], plo[d]);
+        ihi[d] = std::min(brk.origin[d] + brk.dims[d] * brk.h[d], phi[d]);
+      }
+      if (complete) {
+        bool eq = true;
+        for (int d = 0; d < 3; ++d) eq = eq && ilo[d] == plo[d] && ihi[d] == phi[d];
+        *complete = eq;
+      }
+      for (int d = 0; d < 3; ++d)
+        if (ilo[d] >= ihi[d]) return false;
+      int lo[3], hi[3];
+      for (int d = 0; d < 3; ++d) {
+        // brick::index_range (grid.hpp:323-331); the clamp only guards the
+        // arrays against a quotient that rounds past the brick's last cell
+        lo[d] = std::max(0, (int)std::floor((ilo[d] - brk.origin[d]) / brk.h[d]));
+        hi[d] = std::min(brk.dims[d], (int)std::ceil((ihi[d] - brk.origin[d]) / brk.h[d]));
+      }
+      for (int k = lo[2]; k < hi[2]; ++k)
+        for (int jj = lo[1]; jj < hi[1]; ++jj)
+          for (int i = lo[0]; i < hi[0]; ++i) {
+            const int64_t g = brk.start + i + brk.strides[1] * jj + brk.strides[2] * k;
+            for (uint32_t t = cell_starts[g]; t < cell_starts[g + 1]; ++t) {
+              const uint32_t node = cell_nodes[t];
+              const double d[3] = {center[0] - nodes[3 * (size_t)node],
+                                   center[1] - nodes[3 * (size_t)node + 1],
+                                   center[2] - nodes[3 * (size_t)node + 2]};
+              const double val = q[pn] * sf(d);
+              if (rho) rho[node] += val;
+              if (j)
+                for (int a = 0; a < 3; ++a) j[3 * (size_t)node + a] += sfac[a] * val;
+            }
+          }
+      return true;
+    };
+    deposit_periodic_copies(*m, B, sf.radius, x + 3 * pn,
+                            brick_cache ? brick_cache + pn : nullptr, on_brick);
   }
   return 0;
 }

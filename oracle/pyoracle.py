@@ -55,9 +55,12 @@ def lib(parallel: bool = False) -> C.CDLL:
     h.orc_deposit_shape.argtypes = [md, C.c_int, L.ShapeFunctionDesc, _dp, C.c_int64, _dp, _dp,
                                     _dp, _u32p, _dp, _dp, _dp]
     h.orc_walk_elements.argtypes = [md, _dp, C.c_uint32, C.c_double, _u32p, C.c_int]
-    h.orc_deposit_grid.argtypes = [md, C.c_int, C.POINTER(L.Brick), C.c_int,
+    h.orc_deposit_grid.argtypes = [md, C.c_int, C.POINTER(L.Brick), _dp, C.c_int,
                                    L.ShapeFunctionDesc, C.c_int64, _dp, _dp, _dp, C.c_int64,
                                    _dp, _dp, _u32p]
+    h.orc_deposit_grid_find.argtypes = [md, C.c_int, C.POINTER(L.Brick), _u32p, _u32p, _dp,
+                                        C.c_int64, L.ShapeFunctionDesc, C.c_int64, _dp, _dp,
+                                        _dp, _dp, _dp, _u32p]
     h.orc_remap_grid_to_mesh.argtypes = [C.POINTER(L.GridDesc), _dp, _dp, C.c_int64, C.c_int64]
     h.orc_pic_steps_parallel.argtypes = [C.c_void_p, md, C.c_int64, _dp, _dp, _dp, _dp, _u32p,
                                          _dp, _dp, C.POINTER(_dp), C.c_int, _dp, _dp,
@@ -195,16 +198,38 @@ def walk_elements(om: OracleMesh, pos, start, radius, cap=100000):
 
 
 def deposit_grid(om: OracleMesh, bricks, weights, shape, x, q, v, gnc, rho=True, j=True,
-                 brick_cache=None):
+                 brick_cache=None, point_origins=None):
+    """point_origins: [bricks, 3, 3] for jiggly bricks, or None."""
     arr = (L.Brick * len(bricks))(*bricks)
     r = np.empty(gnc) if rho else None
     jj = np.empty((gnc, 3)) if j else None
     cache = np.zeros(len(x), dtype=np.uint32) if brick_cache is None else brick_cache
     sd = L.ShapeFunctionDesc(shape.radius, shape.alpha, shape.normalizer)
-    lib().orc_deposit_grid(om.ref, len(bricks), arr, weights, sd, len(x),
+    po = None if point_origins is None else np.ascontiguousarray(point_origins, dtype=np.float64)
+    lib().orc_deposit_grid(om.ref, len(bricks), arr, _p(po), weights, sd, len(x),
                            _p(np.ascontiguousarray(x)), _p(np.ascontiguousarray(q)),
                            _p(None if v is None else np.ascontiguousarray(v)), gnc, _p(r), _p(jj),
                            _p(cache, C.c_uint32))
+    return r, jj
+
+
+def deposit_grid_find(om: OracleMesh, bricks, cell_starts, cell_nodes, nodes, shape, x, q, v,
+                      rho=True, j=True, brick_cache=None):
+    """GridFindDepositor: rho [Nn], j [Nn, 3] through the brick cells' node
+    lists (cell_starts [G+1], cell_nodes)."""
+    arr = (L.Brick * len(bricks))(*bricks)
+    nn = len(nodes)
+    r = np.empty(nn) if rho else None
+    jj = np.empty((nn, 3)) if j else None
+    cache = np.zeros(len(x), dtype=np.uint32) if brick_cache is None else brick_cache
+    sd = L.ShapeFunctionDesc(shape.radius, shape.alpha, shape.normalizer)
+    cs = np.ascontiguousarray(cell_starts, dtype=np.uint32)
+    cn = np.ascontiguousarray(cell_nodes, dtype=np.uint32)
+    lib().orc_deposit_grid_find(om.ref, len(bricks), arr, _p(cs, C.c_uint32), _p(cn, C.c_uint32),
+                                _p(np.ascontiguousarray(nodes, dtype=np.float64)), nn, sd, len(x),
+                                _p(np.ascontiguousarray(x)), _p(np.ascontiguousarray(q)),
+                                _p(None if v is None else np.ascontiguousarray(v)), _p(r), _p(jj),
+                                _p(cache, C.c_uint32))
     return r, jj
 
 

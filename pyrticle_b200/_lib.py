@@ -120,6 +120,7 @@ class GridDesc(C.Structure):
         ("avg_group_count", C.c_int64),
         ("avg_group_starts", _u32p),
         ("avg_group_nodes", _u32p),
+        ("point_origins", _dp),
     ]
 
 

@@ -7,6 +7,8 @@
 // the tile's bounding sphere. Weights: the shape function at the point (the
 // reference's grid depositor) or trilinear weights (cell-centred hat
 // functions, clamped at the brick edge so that they always sum to one).
+// Jiggly bricks (grid.hpp:345-449) take their points from three jittered
+// point origins; the tile boxes grow by the largest jitter.
 
 #include <cub/cub.cuh>
 
@@ -27,10 +29,18 @@ using namespace prt_dep;
 
 // ---------------------------------------------------------------- targets
 
+// Per brick of a jiggly grid: the three point origins and, per axis, the
+// largest distance of a point from its cell centre.
+struct JiggleDev {
+  double origins[3][3];
+  double pad[3];
+};
+
 // Tile of 8 x 4 x 4 points of one brick; one group (the tile box).
 struct BrickTarget {
   const prt_brick *__restrict__ bricks;
   const long long *__restrict__ tile_starts;  // [bricks+1] cumulative tile counts
+  const JiggleDev *__restrict__ jiggle;       // [bricks] or NULL (regular points)
   int brick_count;
   int check_tag;
 
@@ -69,6 +79,14 @@ struct BrickTarget {
     int b, idx[3];
     valid(tile, t, b, idx);
     const prt_brick &B = bricks[b];
+    if (jiggle) {
+      // jiggly_brick::point (grid.hpp:386-396)
+      const double *o = jiggle[b].origins[(idx[0] + idx[1] + idx[2]) % 3];
+      x0 = o[0] + idx[0] * B.stepwidths[0];
+      x1 = o[1] + idx[1] * B.stepwidths[1];
+      x2 = o[2] + idx[2] * B.stepwidths[2];
+      return;
+    }
     x0 = B.origin[0] + B.stepwidths[0] / 2 + idx[0] * B.stepwidths[0];
     x1 = B.origin[1] + B.stepwidths[1] / 2 + idx[1] * B.stepwidths[1];
     x2 = B.origin[2] + B.stepwidths[2] / 2 + idx[2] * B.stepwidths[2];
@@ -83,6 +101,10 @@ struct BrickTarget {
       int last = min(i0[d] + cnt, B.dims[d]) - 1;
       lo[d] = B.origin[d] + B.stepwidths[d] / 2 + i0[d] * B.stepwidths[d];
       hi[d] = B.origin[d] + B.stepwidths[d] / 2 + last * B.stepwidths[d];
+      if (jiggle) {
+        lo[d] -= jiggle[b].pad[d];
+        hi[d] += jiggle[b].pad[d];
+      }
     }
   }
   __device__ void group_sphere(long long tile, int, double radius, double s[4]) const {
@@ -321,6 +343,7 @@ struct prt_grid {
   int np;
   std::vector<prt_brick> host_bricks;
   prt_brick *bricks = nullptr;
+  JiggleDev *jiggle = nullptr;
   long long *tile_starts = nullptr;
   long long tiles = 0;
   long long grid_nodes = 0;
@@ -372,6 +395,26 @@ extern "C" int prt_grid_create(const prt_mesh *mesh, const prt_grid_desc *d, prt
   };
   int rc = up(&g->bricks, d->bricks, d->brick_count);
   if (!rc) rc = up(&g->tile_starts, ts.data(), ts.size());
+  if (!rc && d->point_origins) {
+    std::vector<JiggleDev> jg(d->brick_count);
+    for (int b = 0; b < d->brick_count && !rc; ++b) {
+      const prt_brick &B = d->bricks[b];
+      for (int a = 0; a < 3; ++a) {
+        const double centre = B.origin[a] + B.stepwidths[a] / 2;
+        double pad = 0;
+        for (int i = 0; i < 3; ++i) {
+          const double o = d->point_origins[9 * b + 3 * i + a];
+          jg[b].origins[i][a] = o;
+          pad = std::max(pad, std::fabs(o - centre));
+        }
+        // points stay within their cells (the reference's index ranges
+        // assume it); the margin covers the rounding of idx * h
+        if (!(pad <= 0.5 * B.stepwidths[a] * (1 + 1e-12))) rc = PRT_ERR_INVALID_ARGUMENT;
+        jg[b].pad[a] = pad * (1 + 1e-9) + 1e-12 * B.stepwidths[a];
+      }
+    }
+    if (!rc) rc = up(&g->jiggle, jg.data(), jg.size());
+  }
   g->eog_count = d->eog_count;
   if (d->eog_count > 0) {
     // one element-on-grid per element: the remap owns its nodes
@@ -409,7 +452,7 @@ extern "C" int prt_grid_create(const prt_mesh *mesh, const prt_grid_desc *d, prt
 
 extern "C" int prt_grid_destroy(prt_grid *g) {
   if (!g) return PRT_OK;
-  void *ptrs[] = {g->bricks, g->tile_starts, g->eog_elements, g->eog_starts, g->eog_nodes,
+  void *ptrs[] = {g->bricks, g->tile_starts, g->jiggle, g->eog_elements, g->eog_starts, g->eog_nodes,
                   g->eog_weights, g->eog_mstarts, g->eog_matrices, g->avg_starts, g->avg_nodes};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -443,6 +486,7 @@ extern "C" int prt_deposit_grid(const prt_grid *g, prt_workspace *ws, int32_t we
   if (!g || !ws || n < 0 || n >= (1ll << 31)) return PRT_ERR_INVALID_ARGUMENT;
   if (weights != PRT_GRID_SHAPE && weights != PRT_GRID_TRILINEAR) return PRT_ERR_INVALID_ARGUMENT;
   if (weights == PRT_GRID_SHAPE && !(shape.radius > 0)) return PRT_ERR_INVALID_ARGUMENT;
+  if (weights == PRT_GRID_TRILINEAR && g->jiggle) return PRT_ERR_INVALID_ARGUMENT;
   if (n > 0 && (!x || !q || (grid_j && !v))) return PRT_ERR_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;
   const long long G_n = g->grid_nodes;
@@ -515,6 +559,7 @@ extern "C" int prt_deposit_grid(const prt_grid *g, prt_workspace *ws, int32_t we
   BrickTarget T;
   T.bricks = g->bricks;
   T.tile_starts = g->tile_starts;
+  T.jiggle = g->jiggle;
   T.brick_count = g->brick_count;
   T.check_tag = weights == PRT_GRID_TRILINEAR;
   if (grid_rho) PRT_CHECK_CUDA(cudaMemsetAsync(grid_rho, 0, G_n * sizeof(double), s));

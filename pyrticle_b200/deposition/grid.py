@@ -72,6 +72,85 @@ class BrickInfo:
         return b
 
 
+class MT19937:
+    """The 32-bit Mersenne Twister (Matsumoto and Nishimura, 1998), the
+    engine of the reference's jiggly bricks (boost::mt19937, default seed
+    5489). Known answer: the 10000th output from the default seed is
+    4123659995."""
+
+    def __init__(self, seed=5489):
+        self.mt = [0] * 624
+        self.mt[0] = seed & 0xFFFFFFFF
+        for i in range(1, 624):
+            prev = self.mt[i - 1]
+            self.mt[i] = (1812433253 * (prev ^ (prev >> 30)) + i) & 0xFFFFFFFF
+        self.index = 624
+
+    def _twist(self):
+        mt = self.mt
+        for i in range(624):
+            y = (mt[i] & 0x80000000) | (mt[(i + 1) % 624] & 0x7FFFFFFF)
+            v = mt[(i + 397) % 624] ^ (y >> 1)
+            if y & 1:
+                v ^= 0x9908B0DF
+            mt[i] = v
+        self.index = 0
+
+    def __call__(self):
+        if self.index >= 624:
+            self._twist()
+        y = self.mt[self.index]
+        self.index += 1
+        y ^= y >> 11
+        y ^= (y << 7) & 0x9D2C5680
+        y ^= (y << 15) & 0xEFC60000
+        y ^= y >> 18
+        return y & 0xFFFFFFFF
+
+
+def uniform_real(engine, lo, hi):
+    """boost::uniform_real<>(lo, hi) over a 32-bit engine:
+    lo + (hi - lo) * k / 2^32 for the engine's output k."""
+    return float(engine()) / 4294967296.0 * (hi - lo) + lo
+
+
+class JigglyBrickInfo(BrickInfo):
+    """A brick whose points are jittered (grid.hpp:345-449): three point
+    origins origin + h/2 + offset_i, offset_i = U(-r, r) * h per axis drawn
+    from a fresh MT19937 (i outer, axis inner), and point idx taking origin
+    (i + j + k) % 3. Every brick draws the same offsets (in cell units).
+
+    The reference's jiggly iterator advances along x by the offset of the
+    origin after the next one, so the points it visits along a row depend on
+    where the row starts; this build uses point(idx) everywhere (setup and
+    deposition), which is the brick's own definition of its points."""
+
+    def __init__(self, number, start_index, stepwidths, origin, dims, jiggle_radius):
+        BrickInfo.__init__(self, number, start_index, stepwidths, origin, dims)
+        if not 0 < jiggle_radius <= 0.5:
+            # beyond half a cell a point can leave its cell, and the index
+            # ranges the reference walks would miss points within the radius
+            raise ValueError("jiggle_radius must be in (0, 0.5]")
+        self.jiggle_radius = float(jiggle_radius)
+        eng = MT19937()
+        oph = self.origin + self.stepwidths / 2
+        po = np.empty((3, 3))
+        for i in range(3):
+            for a in range(3):
+                po[i, a] = uniform_real(eng, -jiggle_radius, jiggle_radius) * self.stepwidths[a]
+            po[i] = oph + po[i]
+        self.point_origins = po
+
+    def point(self, idx):
+        idx = np.asarray(idx)
+        return self.point_origins[int(idx.sum()) % 3] + idx * self.stepwidths
+
+    def points(self, idx):
+        """point() of an [..., 3] index array."""
+        idx = np.asarray(idx)
+        return self.point_origins[idx.sum(axis=-1) % 3] + idx * self.stepwidths
+
+
 def find_points_in_elements(mesh, bricks, el_tolerance, chunk=20000):
     """Per element, the grid points within the tolerance-grown element
     (dep_grid.hpp:142-213). Returns (starts[E+1], grid_index, points, weights)."""
@@ -106,7 +185,10 @@ def find_points_in_elements(mesh, bricks, el_tolerance, chunk=20000):
                             oz.transpose(2, 1, 0).ravel()], axis=1)      # [K, 3]
             idx = lo_i[sl][:, None, :] + off[None]                          # [e, K, 3]
             valid = np.all(off[None] < ext[sl][:, None, :], axis=2)
-            pts = brk.origin + brk.stepwidths / 2 + idx * brk.stepwidths   # [e, K, 3]
+            if isinstance(brk, JigglyBrickInfo):
+                pts = brk.points(idx)
+            else:
+                pts = brk.origin + brk.stepwidths / 2 + idx * brk.stepwidths   # [e, K, 3]
             n = mesh.face_normals[sl]                                       # [e, 4, 3]
             rhs = mesh.face_plane_rhs[sl]
             dist = np.einsum("eki,efi->ekf", pts, n) - rhs[:, None, :]
@@ -227,15 +309,18 @@ class GridDepositor(Depositor):
         self.submethod = submethod
         if submethod != "simplex_reduce":
             raise NotImplementedError("only submethod='simplex_reduce' (the reference default)")
-        if filter_min_amplification is not None or jiggle_radius:
-            raise NotImplementedError("filters and jiggly bricks are not supported")
+        if filter_min_amplification is not None:
+            raise NotImplementedError("DG filters are not supported")
         if grid_weights not in ("shape", "trilinear"):
             raise ValueError("grid_weights must be 'shape' or 'trilinear'")
+        if jiggle_radius and grid_weights != "shape":
+            raise ValueError("trilinear weights need the regular cell-centred points")
+        self.jiggle_radius = jiggle_radius
         self.grid_weights = grid_weights
 
     @property
     def name(self):
-        return "GridRegular"
+        return "GridJiggly" if self.jiggle_radius else "GridRegular"
 
     def initialize(self, method):
         Depositor.initialize(self, method)
@@ -243,7 +328,10 @@ class GridDepositor(Depositor):
         self.bricks = []
         start = 0
         for i, (sw, origin, dims) in enumerate(self.brick_generator(discr)):
-            b = BrickInfo(i, start, sw, origin, dims)
+            if self.jiggle_radius:
+                b = JigglyBrickInfo(i, start, sw, origin, dims, self.jiggle_radius)
+            else:
+                b = BrickInfo(i, start, sw, origin, dims)
             self.bricks.append(b)
             start += len(b)
         self.grid_node_count = start
@@ -274,6 +362,9 @@ class GridDepositor(Depositor):
         d.eog_matrix_starts = _lib.ptr(arr(mstarts, np.uint64), C.c_uint64)
         d.eog_matrices = _lib.ptr(arr(mats, np.float64))
         d.avg_group_count = 0
+        if self.jiggle_radius:
+            d.point_origins = _lib.ptr(arr(np.stack([b.point_origins for b in self.bricks]),
+                                           np.float64))
         self.grid_desc = d
         self._keep = keep
         h = C.c_void_p()
