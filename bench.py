@@ -230,7 +230,29 @@ def form_accuracy(m, s, fields, dt, torch, steps=5):
     out[f"x_rel_l2_after_{steps}_steps"] = rel(x32, x64)
     out[f"dp_rel_l2_after_{steps}_steps"] = rel(p32 - s.p, p64 - s.p)
     out["elements_equal_fraction"] = float((el32 == el64).float().mean())
+    del x64, p64, el64, x32, p32, el32
     m.check_status()
+    out["normalized_total_charge_rel_error"] = normalized_charge(m, s, torch)
+    return out
+
+
+def normalized_charge(m, s, torch):
+    """|sum_e |J_e| sum_i w_i rho_i - sum_p q_p| / |sum_p q_p| of the
+    normalising depositor on the same state: FP64 (the form the normalised
+    depositor keeps in the chosen configuration) and FP32 weights."""
+    from pyrticle_b200.deposition.shape import NormalizedShapeFunctionDepositor
+    dep = NormalizedShapeFunctionDepositor()
+    dep.initialize(m)
+    dep.set_shape_function(None, m.depositor.shape_function)
+    iw = torch.as_tensor(dep.integral_weights, device=s.x.device)
+    jac = torch.as_tensor(m.discretization.mesh.jacobians, device=s.x.device)
+    qsum = float(s.q.sum())
+    out = {}
+    for prec in ("fp64", "mixed"):
+        rho, _ = dep.deposit_densities_device(s, j=False, precision=prec)
+        total = float(((rho.view(-1, iw.shape[0]) @ iw) * jac).sum())
+        out[prec] = abs(total - qsum) / abs(qsum)
+        del rho
     return out
 
 

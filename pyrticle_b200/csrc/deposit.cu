@@ -208,20 +208,30 @@ constexpr int RING = 64;
 // Streams the candidate particles of one warp's position group: the
 // particles of the bin rows that can come within `radius` of the group's box
 // [c + lo, c + hi], 32 at a time (one per lane, straight from L2/L1). Calls
-// visit(in, k, w0, w1, w2, d2) on every lane for every batch (warp-uniform),
+// visit(in, k, w0, w1, w2) on every lane for every batch (warp-uniform),
 // with w the particle's position relative to c (periodic images shifted by
-// the period), d2 = |w|^2 and `in` set when the particle lies within the
-// radius of the box, hence possibly within the radius of a position.
+// the period) and `in` set when the particle may lie within the radius of
+// the box (never cleared for one that does), hence possibly within the
+// radius of a position.
 template <class Visit>
 __device__ __forceinline__ void stream_box(const BinGrid &G, const DepParticles &P,
                                            const double c[3], const double lo[3],
                                            const double hi[3], double radius, int lane,
                                            Visit &&visit) {
-  const double rc = radius * (1 + 1e-9), rc2 = rc * rc;
-  const double rr = radius * (1 + 1e-6), rr2 = rr * rr;
+  // The culls only decide which particles are evaluated (a particle beyond
+  // the radius gets weight 0 anyway), so they run on few registers: the box
+  // as FP32 centre and half-extent (relative to c) grown by 1e-5 of the
+  // radius, which covers their FP32 rounding, and the per-particle test in
+  // FP32 on the FP64 offsets rounded to FP32.
+  const double rr = radius * (1 + 1e-5), rr2 = rr * rr;
+  const float rcf = (float)rr;
+  const float rc4 = 4.0f * rcf * rcf;
+  float midf[3], halff[3];
   int ulo[3], uhi[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
+    midf[d] = (float)(0.5 * (lo[d] + hi[d]));
+    halff[d] = (float)(0.5 * (hi[d] - lo[d]) + 1e-5 * radius);
     ulo[d] = bin_floor(G, d, c[d] + lo[d] - radius);
     uhi[d] = bin_floor(G, d, c[d] + hi[d] + radius);
     if (G.periodic[d]) {
@@ -233,16 +243,10 @@ __device__ __forceinline__ void stream_box(const BinGrid &G, const DepParticles 
     }
   }
   const double2 *__restrict__ pay = reinterpret_cast<const double2 *>(P.payload);
-  double mid[3], half[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    mid[d] = 0.5 * (lo[d] + hi[d]);
-    half[d] = 0.5 * (hi[d] - lo[d]);
-  }
   // distance from the slab [blo, blo + w) of bins to the box along one axis
   auto slab_gap = [&](int d, double blo) {
-    const double e = fmax(0.0, fmax(blo - (c[d] + hi[d]), (c[d] + lo[d]) - (blo + G.w[d]))) -
-                     G.slack[d];
+    const double m = c[d] + (double)midf[d], h = (double)halff[d];
+    const double e = fmax(0.0, fmax(blo - (m + h), (m - h) - (blo + G.w[d]))) - G.slack[d];
     return e > 0 ? e * e : 0.0;
   };
   for (int bz = ulo[2]; bz <= uhi[2]; ++bz) {
@@ -258,8 +262,9 @@ __device__ __forceinline__ void stream_box(const BinGrid &G, const DepParticles 
       const double dyz2 = dz2 + slab_gap(1, G.origin[1] + by * G.w[1]);
       if (dyz2 > rr2) continue;
       const double rem = sqrt(rr2 - dyz2);
-      int bx0 = bin_floor(G, 0, c[0] + lo[0] - rem);
-      int bx1 = bin_floor(G, 0, c[0] + hi[0] + rem);
+      const double m0 = c[0] + (double)midf[0], h0 = (double)halff[0];
+      int bx0 = bin_floor(G, 0, m0 - h0 - rem);
+      int bx1 = bin_floor(G, 0, m0 + h0 + rem);
       if (G.periodic[0]) {
         bx0 -= 1;
         bx1 += 1;
@@ -282,21 +287,20 @@ __device__ __forceinline__ void stream_box(const BinGrid &G, const DepParticles 
         for (uint32_t b0 = s0; b0 < s1; b0 += 32) {
           const uint32_t k = b0 + lane;
           bool in = false;
-          double w0 = 0, w1 = 0, w2 = 0, d2 = 0;
+          double w0 = 0, w1 = 0, w2 = 0;
           if (k < s1) {
             const double2 xy = pay[4 * (size_t)k], zq = pay[4 * (size_t)k + 1];
             w0 = xy.x + sx;
             w1 = xy.y + sy;
             w2 = zq.x + sz;
-            d2 = w0 * w0 + w1 * w1 + w2 * w2;
             // per axis 2 max(|w - mid| - half, 0) = d + |d|
-            const double d0 = fabs(w0 - mid[0]) - half[0];
-            const double d1 = fabs(w1 - mid[1]) - half[1];
-            const double d2a = fabs(w2 - mid[2]) - half[2];
-            const double e0 = d0 + fabs(d0), e1 = d1 + fabs(d1), e2 = d2a + fabs(d2a);
-            in = e0 * e0 + e1 * e1 + e2 * e2 <= 4 * rc2;
+            const float d0 = fabsf((float)w0 - midf[0]) - halff[0];
+            const float d1 = fabsf((float)w1 - midf[1]) - halff[1];
+            const float d2a = fabsf((float)w2 - midf[2]) - halff[2];
+            const float e0 = d0 + fabsf(d0), e1 = d1 + fabsf(d1), e2 = d2a + fabsf(d2a);
+            in = e0 * e0 + e1 * e1 + e2 * e2 <= rc4;
           }
-          visit(in, k, w0, w1, w2, d2);
+          visit(in, k, w0, w1, w2);
         }
       }
     }
@@ -450,9 +454,10 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
   warp_box<PPL>(pos, p0, npg, lane, cc, blo, bhi);
   const double2 *__restrict__ pay = reinterpret_cast<const double2 *>(P.payload);
   stream_box(G, P, cc, blo, bhi, S.radius, lane,
-             [&](bool in, uint32_t k, double w0, double w1, double w2, double d2) {
+             [&](bool in, uint32_t k, double w0, double w1, double w2) {
                const unsigned bal = __ballot_sync(0xffffffffu, in);
                if (in) {
+                 const double d2 = w0 * w0 + w1 * w1 + w2 * w2;
                  const double2 zq = pay[4 * (size_t)k + 1];
                  const double2 jv = pay[4 * (size_t)k + 2], jt = pay[4 * (size_t)k + 3];
                  const int slot =
@@ -507,6 +512,10 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
                                 DepParticles P, ShapeParams S, long long npos,
                                 double *__restrict__ out) {
   __shared__ float4 ring[WARPS][2][RING];
+  // per lane its positions' FP64 sums (rho, j_x, j_y, j_z per position),
+  // kept in shared memory: registers go to the streaming state and the
+  // batch arithmetic
+  __shared__ double acc64[WARPS][4 * PPL][32];
 
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const long long g = blockIdx.x * (long long)WARPS + wid;
@@ -514,6 +523,7 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
   const uint32_t p0 = gstarts[g];
   const int npg = (int)(gstarts[g + 1] - p0);
   float4(*R)[RING] = ring[wid];
+  double(*A64)[32] = acc64[wid];
 
   const double c0 = gspheres[4 * g], c1 = gspheres[4 * g + 1], c2 = gspheres[4 * g + 2];
   // lane holds positions p0 + lane + 32 h, h < PPL; the weight base
@@ -534,9 +544,8 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
       V2[h] = (float)(2 * u2 * S.inv_radius);
     }
   }
-  double r64[PPL], x64[PPL], y64[PPL], z64[PPL];
 #pragma unroll
-  for (int h = 0; h < PPL; ++h) r64[h] = x64[h] = y64[h] = z64[h] = 0;
+  for (int k = 0; k < 4 * PPL; ++k) A64[k][lane] = 0;
   const float alpha = (float)S.alpha;
   // alpha = 2: (tr + |tr|)^2 = 4 max(tr, 0)^2, the 1/4 applied to the FP64
   // sums at the end (exact)
@@ -559,42 +568,38 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
     }
   };
   // FP32 batch sums into the FP64 accumulators
-  auto combine = [&](const float *ra, const float *xa, const float *ya, const float *za,
-                     const float *rb, const float *xb, const float *yb, const float *zb) {
+  auto combine = [&](const float *ra, const float *xa, const float *ya, const float *za) {
 #pragma unroll
     for (int h = 0; h < PPL; ++h) {
-      r64[h] += (double)ra[h] + (double)rb[h];
-      x64[h] += (double)xa[h] + (double)xb[h];
-      y64[h] += (double)ya[h] + (double)yb[h];
-      z64[h] += (double)za[h] + (double)zb[h];
+      A64[4 * h][lane] += (double)ra[h];
+      A64[4 * h + 1][lane] += (double)xa[h];
+      A64[4 * h + 2][lane] += (double)ya[h];
+      A64[4 * h + 3][lane] += (double)za[h];
     }
   };
   int head = 0, count = 0;
   auto drain = [&](int k) {
-    float ra[PPL], xa[PPL], ya[PPL], za[PPL], rb[PPL], xb[PPL], yb[PPL], zb[PPL];
+    float ra[PPL], xa[PPL], ya[PPL], za[PPL];
 #pragma unroll
-    for (int h = 0; h < PPL; ++h) ra[h] = xa[h] = ya[h] = za[h] = rb[h] = xb[h] = yb[h] = zb[h] = 0;
+    for (int h = 0; h < PPL; ++h) ra[h] = xa[h] = ya[h] = za[h] = 0;
     for (int i = 0; i < k; ++i) {
       const int e = (head + i) & (RING - 1);
       pair(R[0][e], R[1][e], ra, xa, ya, za);
     }
-    combine(ra, xa, ya, za, rb, xb, yb, zb);
+    combine(ra, xa, ya, za);
     head = (head + k) & (RING - 1);
     count -= k;
   };
-  // a full batch of 32 from head (0 or 32): constant offsets, two entries
-  // per step into two sets of FP32 batch sums
+  // a full batch of 32 from head (0 or 32): constant offsets, one set of
+  // FP32 batch sums (4 PPL independent accumulation chains)
   auto drain_full = [&]() {
-    float ra[PPL], xa[PPL], ya[PPL], za[PPL], rb[PPL], xb[PPL], yb[PPL], zb[PPL];
+    float ra[PPL], xa[PPL], ya[PPL], za[PPL];
 #pragma unroll
-    for (int h = 0; h < PPL; ++h) ra[h] = xa[h] = ya[h] = za[h] = rb[h] = xb[h] = yb[h] = zb[h] = 0;
+    for (int h = 0; h < PPL; ++h) ra[h] = xa[h] = ya[h] = za[h] = 0;
     const float4 *E0 = &R[0][head], *E1 = &R[1][head];
 #pragma unroll MIXED_UNROLL
-    for (int i = 0; i < 32; i += 2) {
-      pair(E0[i], E1[i], ra, xa, ya, za);
-      pair(E0[i + 1], E1[i + 1], rb, xb, yb, zb);
-    }
-    combine(ra, xa, ya, za, rb, xb, yb, zb);
+    for (int i = 0; i < 32; ++i) pair(E0[i], E1[i], ra, xa, ya, za);
+    combine(ra, xa, ya, za);
     head = (head + 32) & (RING - 1);
     count -= 32;
   };
@@ -604,9 +609,10 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
   warp_box<PPL>(pos, p0, npg, lane, cc, blo, bhi);
   const double2 *__restrict__ pay = reinterpret_cast<const double2 *>(P.payload);
   stream_box(G, P, cc, blo, bhi, S.radius, lane,
-             [&](bool in, uint32_t k, double w0, double w1, double w2, double d2) {
+             [&](bool in, uint32_t k, double w0, double w1, double w2) {
                const unsigned bal = __ballot_sync(0xffffffffu, in);
                if (in) {
+                 const double d2 = w0 * w0 + w1 * w1 + w2 * w2;
                  const double2 zq = pay[4 * (size_t)k + 1];
                  const double2 jv = pay[4 * (size_t)k + 2], jt = pay[4 * (size_t)k + 3];
                  const int slot =
@@ -627,10 +633,10 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
   for (int h = 0; h < PPL; ++h)
     if (live[h]) {
       const long long u = p0 + lane + 32 * h;
-      out[u] = r64[h] * wscale;
-      out[npos + u] = x64[h] * wscale;
-      out[2 * npos + u] = y64[h] * wscale;
-      out[3 * npos + u] = z64[h] * wscale;
+      out[u] = A64[4 * h][lane] * wscale;
+      out[npos + u] = A64[4 * h + 1][lane] * wscale;
+      out[2 * npos + u] = A64[4 * h + 2][lane] * wscale;
+      out[3 * npos + u] = A64[4 * h + 3][lane] * wscale;
     }
 }
 
