@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "binning.cuh"
+#include "gather.cuh"
 
 namespace prt_dep {
 
@@ -676,63 +677,73 @@ __global__ void position_weights_kernel(long long npos, const uint32_t *__restri
 
 // Normalising pre-pass (dep_normshape.hpp:125-199): per particle the
 // integral of its deposited shape, sum_u W_u N S(x_u - x_p), over the
-// positions within the radius (one warp per particle, position tiles found
-// through uniform tile bins); scale = q / integral, or 0 with a warning for a
-// zero integral (the reference skips such a particle).
+// positions within the radius; scale = q / integral, or 0 with a warning for
+// a zero integral (the reference skips such a particle). A warp takes 32
+// consecutive particles (element-sorted particles are close together), one
+// per lane, and walks the position groups near them with the positions and
+// W staged in shared memory (gather.cuh); each particle's sum runs in a fixed
+// order. hits_out: the positions within the radius (-1 for a dead particle).
+constexpr int NORM_WARPS = 4;
 template <bool ALPHA2>
-__global__ void normalize_kernel(DevMesh M, TileBinsDev TB, const double *__restrict__ pos,
-                                 long long npos, const double *__restrict__ boxes,
-                                 const double *__restrict__ W, ShapeParams S,
-                                 double normalizer, long long n,
-                                 const double *__restrict__ x, const double *__restrict__ q,
-                                 const uint32_t *__restrict__ el,
-                                 double *__restrict__ scale_out,
-                                 double *__restrict__ hits_out, DevStatus *st) {
-  const long long i = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= n) return;
-  if (el && el[i] == PRT_INVALID) {
-    if (lane == 0) {
-      scale_out[i] = 0;
-      hits_out[i] = -1;
-    }
+__global__ void __launch_bounds__(32 * NORM_WARPS)
+    normalize_kernel(DevMesh M, CentreBinsDev CB, const double *__restrict__ pos,
+                     long long npos, const double *__restrict__ W, ShapeParams S,
+                     double normalizer, long long n, const double *__restrict__ x,
+                     const double *__restrict__ q, const uint32_t *__restrict__ el,
+                     double *__restrict__ scale_out, double *__restrict__ hits_out,
+                     DevStatus *st) {
+  __shared__ GatherStage<1> stage[NORM_WARPS];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long w0 = (blockIdx.x * (long long)NORM_WARPS + wid) * 32;
+  if (w0 >= n) return;  // whole warp
+  const long long i = w0 + lane;
+  const bool valid = i < n;
+  const bool live = valid && !(el && el[i] == PRT_INVALID);
+  double p[3] = {0, 0, 0};
+  if (live) {
+    p[0] = x[i];
+    p[1] = x[n + i];
+    p[2] = x[2 * n + i];
+  }
+  double integral = 0, hits = 0;
+  warp_gather_positions<1>(M, CB, pos, npos, W, S.radius, live, p, stage[wid],
+                           [&](double, double, double, double r2, const double *vals) {
+                             const bool in = r2 <= S.radius2;
+                             const double rt = S.radius - r2 * S.inv_radius;
+                             const double sv =
+                                 in ? normalizer * (ALPHA2 ? rt * rt : pow(rt, S.alpha))
+                                    : 0.0;
+                             integral = fma(sv, vals[0], integral);
+                             hits += in ? 1.0 : 0.0;
+                           });
+  if (!valid) return;
+  if (!live) {
+    scale_out[i] = 0;
+    hits_out[i] = -1;
     return;
   }
-  const double px = x[i], py = x[n + i], pz = x[2 * n + i];
-  double integral = 0;
-  double hits = 0;
-  visit_positions_in_reach(M, TB, pos, npos, boxes, S, px, py, pz, lane,
-                           [&](long long uu, double, double, double, double r2) {
-                             const double rt = S.radius - r2 * S.inv_radius;
-                             const double s =
-                                 normalizer * (ALPHA2 ? rt * rt : pow(rt, S.alpha));
-                             integral = fma(s, W[uu], integral);
-                             hits += 1;
-                           });
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    integral += __shfl_xor_sync(0xffffffffu, integral, o);
-    hits += __shfl_xor_sync(0xffffffffu, hits, o);
+  if (integral == 0) {
+    scale_out[i] = 0;
+    record_warning(st, PRT_WARN_ZERO_MASS, i);
+  } else {
+    scale_out[i] = q[i] / integral;
   }
-  if (lane == 0) {
-    if (integral == 0) {
-      scale_out[i] = 0;
-      record_warning(st, PRT_WARN_ZERO_MASS, i);
-    } else {
-      scale_out[i] = q[i] / integral;
-    }
-    hits_out[i] = hits;
-  }
+  hits_out[i] = hits;
 }
 
-// Deterministic single-block reduction of count / sum / sum of squares /
-// min / max of the applied scales (non-zero ones) and of the per-particle
-// position counts (live particles).
-__global__ void stats_kernel(long long n, const double *__restrict__ scale,
-                             const double *__restrict__ hits, double *__restrict__ out) {
+// Count / sum / sum of squares / min / max of the applied scales (non-zero
+// ones) and of the per-particle position counts (live particles): per block
+// partials, then one pass over them in block order (deterministic).
+constexpr int STATS_BLOCKS = 592;  // 4 per SM of a 148-SM B200
+__device__ __forceinline__ double stats_combine(int k, double a, double b) {
+  return (k == 3 || k == 8) ? fmin(a, b) : (k == 4 || k == 9) ? fmax(a, b) : a + b;
+}
+__global__ void __launch_bounds__(256) stats_kernel(long long n, const double *__restrict__ scale,
+                                                    const double *__restrict__ hits,
+                                                    double *__restrict__ partials) {
   __shared__ double sh[10][256];
   double acc[10] = {0, 0, 0, INFINITY, -INFINITY, 0, 0, 0, INFINITY, -INFINITY};
-  for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += 256LL * gridDim.x) {
     const double c = hits[i];
     if (c < 0) continue;
     acc[5] += 1;
@@ -752,13 +763,19 @@ __global__ void stats_kernel(long long n, const double *__restrict__ scale,
   __syncthreads();
   for (int o = 128; o > 0; o >>= 1) {
     if ((int)threadIdx.x < o)
-      for (int k = 0; k < 10; ++k) {
-        const double a = sh[k][threadIdx.x], b = sh[k][threadIdx.x + o];
-        sh[k][threadIdx.x] = (k == 3 || k == 8) ? fmin(a, b) : (k == 4 || k == 9) ? fmax(a, b) : a + b;
-      }
+      for (int k = 0; k < 10; ++k)
+        sh[k][threadIdx.x] = stats_combine(k, sh[k][threadIdx.x], sh[k][threadIdx.x + o]);
     __syncthreads();
   }
-  if (threadIdx.x < 10) out[threadIdx.x] = sh[threadIdx.x][0];
+  if (threadIdx.x < 10) partials[10 * (size_t)blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+__global__ void stats_final_kernel(int blocks, const double *__restrict__ partials,
+                                   double *__restrict__ out) {
+  const int k = threadIdx.x;
+  if (k >= 10) return;
+  double a = partials[k];
+  for (int b = 1; b < blocks; ++b) a = stats_combine(k, a, partials[10 * (size_t)b + k]);
+  out[k] = a;
 }
 
 inline uint64_t spread_bits(uint64_t v) {  // 21 bits -> every third bit
@@ -1059,8 +1076,9 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
   if (mode == PRT_DEPOSIT_NORMALIZED) {
     double *sc = (double *)ws_buffer(ws, PRT_WS_DEP_SCALE, 2 * sizeof(double) * (size_t)n, &rc);
     if (!sc) return rc;
-    double *aux = (double *)ws_buffer(ws, PRT_WS_DEP_STATS,
-                                      sizeof(double) * (64 + mesh->dev.Np + PS.count), &rc);
+    double *aux = (double *)ws_buffer(
+        ws, PRT_WS_DEP_STATS,
+        sizeof(double) * (64 + mesh->dev.Np + PS.count + 10 * STATS_BLOCKS), &rc);
     if (!aux) return rc;
     double *iwd = aux + 16, *W = aux + 64 + mesh->dev.Np;
     PRT_CHECK_CUDA(cudaMemcpyAsync(iwd, iw, sizeof(double) * mesh->dev.Np,
@@ -1068,26 +1086,24 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
     position_weights_kernel<<<prt_grid_blocks(PS.count, 256), 256, 0, s>>>(
         PS.count, PS.run_starts, PS.run_nodes, mesh->dev.Np, iwd, mesh->dev.jacobians, W);
     PRT_CHECK_CUDA(cudaGetLastError());
-    TileBinsDev TB;
-    for (int d = 0; d < 3; ++d) {
-      TB.origin[d] = PS.bins.origin[d];
-      TB.inv_w[d] = PS.bins.inv_w[d];
-      TB.dims[d] = PS.bins.dims[d];
-    }
-    TB.starts = PS.bins.starts;
-    TB.tiles = PS.bins.tiles;
-    const long long threads = 32 * (long long)n;
+    const CentreBinsDev CB = centre_bins_dev(PS);
+    const unsigned nblk = (unsigned)((n + 32 * NORM_WARPS - 1) / (32 * NORM_WARPS));
     if (a2)
-      normalize_kernel<true><<<prt_grid_blocks(threads, 128), 128, 0, s>>>(
-          mesh->dev, TB, PS.pos, PS.count, PS.tile_boxes, W, S, shape.normalizer, n, x, q, el,
-          sc, sc + n, ws->status);
+      normalize_kernel<true><<<nblk, 32 * NORM_WARPS, 0, s>>>(
+          mesh->dev, CB, PS.pos, PS.count, W, S, shape.normalizer, n, x, q, el, sc, sc + n,
+          ws->status);
     else
-      normalize_kernel<false><<<prt_grid_blocks(threads, 128), 128, 0, s>>>(
-          mesh->dev, TB, PS.pos, PS.count, PS.tile_boxes, W, S, shape.normalizer, n, x, q, el,
-          sc, sc + n, ws->status);
+      normalize_kernel<false><<<nblk, 32 * NORM_WARPS, 0, s>>>(
+          mesh->dev, CB, PS.pos, PS.count, W, S, shape.normalizer, n, x, q, el, sc, sc + n,
+          ws->status);
     PRT_CHECK_CUDA(cudaGetLastError());
     if (stats) {
-      stats_kernel<<<1, 256, 0, s>>>(n, sc, sc + n, aux);
+      const long long need = (n + 255) / 256;
+      const int sb = (int)(need < STATS_BLOCKS ? need : STATS_BLOCKS);
+      double *partials = W + PS.count;
+      stats_kernel<<<sb, 256, 0, s>>>(n, sc, sc + n, partials);
+      PRT_CHECK_CUDA(cudaGetLastError());
+      stats_final_kernel<<<1, 32, 0, s>>>(sb, partials, aux);
       PRT_CHECK_CUDA(cudaGetLastError());
       double h[10];
       PRT_CHECK_CUDA(cudaMemcpyAsync(h, aux, sizeof(h), cudaMemcpyDeviceToHost, s));
