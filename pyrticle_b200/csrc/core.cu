@@ -141,8 +141,8 @@ extern "C" int prt_mesh_destroy(prt_mesh *m) {
                         m->dev.el_verts, m->dev.verts, m->dev.vadj_starts,
                         m->dev.vadj, m->dev.nodes, m->dev.bin_starts,
                         m->dev.bin_elements, m->face_centroids, m->face_radii,
-                        P.pos, P.node_to_pos, P.run_starts, P.run_nodes, P.tile_boxes,
-                        P.group_starts, P.group_spheres, P.bins.starts, P.bins.tiles,
+                        P.pos, P.node_to_pos, P.run_starts, P.run_nodes,
+                        P.group_starts, P.group_spheres,
                         P.centre_bins.starts, P.centre_bins.spheres, P.centre_bins.ranges,
                         P.wide_starts, P.wide_spheres};
   for (const void *p : ptrs)

@@ -867,26 +867,6 @@ int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
   if ((rc = upload_vec(run_starts, &P.run_starts))) return rc;
   if ((rc = upload_vec(order, &P.run_nodes))) return rc;
 
-  // tiles of PRT_NODE_TILE consecutive positions with their bounding boxes
-  const long long tiles = (npos + PRT_NODE_TILE - 1) / PRT_NODE_TILE;
-  std::vector<double> boxes(6 * (size_t)tiles);
-  double mean_ext[3] = {0, 0, 0};
-  for (long long t = 0; t < tiles; ++t) {
-    double *b = &boxes[6 * t];
-    for (int a = 0; a < 3; ++a) {
-      b[a] = INFINITY;
-      b[3 + a] = -INFINITY;
-    }
-    for (long long p = t * PRT_NODE_TILE; p < std::min(npos, (t + 1) * PRT_NODE_TILE); ++p)
-      for (int a = 0; a < 3; ++a) {
-        b[a] = std::min(b[a], pos[3 * p + a]);
-        b[3 + a] = std::max(b[3 + a], pos[3 * p + a]);
-      }
-    for (int a = 0; a < 3; ++a) mean_ext[a] += b[3 + a] - b[a];
-  }
-  P.tiles = tiles;
-  if ((rc = upload_vec(boxes, &P.tile_boxes))) return rc;
-
   // warp groups: runs of at most 32 positions, cut wherever the Morton cell
   // of about PRT_GROUP_TARGET positions changes, so that no group straddles
   // two cells (compact groups, tight spheres)
@@ -991,48 +971,6 @@ int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
     if ((rc = upload_vec(crange, &CB.ranges))) return rc;
   }
 
-  // uniform bins of about one tile listing the tiles whose box meets them
-  TileBinsHost &H = P.bins;
-  long long nb = 1;
-  for (int a = 0; a < 3; ++a) {
-    const double me = std::max(mean_ext[a] / std::max<long long>(1, tiles), 1e-300);
-    const double e = m->box_hi[a] - m->box_lo[a];
-    const int dims = e > 0 ? (int)std::max(1.0, std::min(512.0, std::floor(e / me))) : 1;
-    H.dims[a] = dims;
-    H.origin[a] = m->box_lo[a];
-    H.inv_w[a] = e > 0 ? dims / e : 0.0;
-    nb *= dims;
-  }
-  auto brange = [&](long long t, int a, int &b0, int &b1) {
-    const double l = std::floor((boxes[6 * t + a] - H.origin[a]) * H.inv_w[a]);
-    const double h = std::floor((boxes[6 * t + 3 + a] - H.origin[a]) * H.inv_w[a]);
-    b0 = (int)std::max(0.0, std::min(l, H.dims[a] - 1.0));
-    b1 = (int)std::max(0.0, std::min(h, H.dims[a] - 1.0));
-  };
-  std::vector<uint32_t> counts(nb + 1, 0), list;
-  for (int pass = 0; pass < 2; ++pass) {
-    std::vector<uint32_t> fill;
-    if (pass == 1) {
-      for (long long b = 0; b < nb; ++b) counts[b + 1] += counts[b];
-      list.resize(counts[nb]);
-      fill.assign(counts.begin(), counts.end() - 1);
-    }
-    for (long long t = 0; t < tiles; ++t) {
-      int r0[3], r1[3];
-      for (int a = 0; a < 3; ++a) brange(t, a, r0[a], r1[a]);
-      for (int z = r0[2]; z <= r1[2]; ++z)
-        for (int y = r0[1]; y <= r1[1]; ++y)
-          for (int x = r0[0]; x <= r1[0]; ++x) {
-            const long long b = x + (long long)H.dims[0] * (y + (long long)H.dims[1] * z);
-            if (pass == 0)
-              ++counts[b + 1];
-            else
-              list[fill[b]++] = (uint32_t)t;
-          }
-    }
-  }
-  if ((rc = upload_vec(counts, &H.starts))) return rc;
-  if ((rc = upload_vec(list, &H.tiles))) return rc;
   return PRT_OK;
 }
 

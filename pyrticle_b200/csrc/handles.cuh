@@ -26,15 +26,6 @@ enum {
   PRT_WS_SLOTS
 };
 
-// Uniform bins over the mesh box listing the position tiles that overlap
-// each bin (used by the particle-centric normalising pass).
-struct TileBinsHost {
-  double origin[3], inv_w[3];
-  int dims[3];
-  const uint32_t *starts = nullptr;
-  const uint32_t *tiles = nullptr;
-};
-
 // Distinct node positions (coincident DG nodes merged), in Morton order:
 // the targets of the mesh deposition.
 struct PositionSet {
@@ -43,9 +34,6 @@ struct PositionSet {
   const uint32_t *node_to_pos = nullptr;  // [Nn]
   const uint32_t *run_starts = nullptr;   // [count + 1] into run_nodes
   const uint32_t *run_nodes = nullptr;    // [Nn] node ids grouped by position, ascending
-  long long tiles = 0;                    // ceil(count / PRT_NODE_TILE)
-  const double *tile_boxes = nullptr;     // [tiles][6]: lo xyz, hi xyz
-  TileBinsHost bins;
   // warp groups: runs of <= 32 consecutive positions that never straddle a
   // Morton cell of about 24 positions, with their bounding spheres
   long long groups = 0;
@@ -125,7 +113,6 @@ int launch_stage_mixed(const prt_pusher *P, prt_workspace *ws, long long n, doub
                        double *kp, const Fields6 &F, double a, double b, double dt, double c,
                        cudaStream_t s);
 
-constexpr int PRT_NODE_TILE = 128;
 constexpr int PRT_WARP_NODES = 32;
 // target positions per Morton cell when cutting warp groups
 constexpr double PRT_GROUP_TARGET = 24.0;
