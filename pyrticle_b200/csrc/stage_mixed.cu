@@ -21,7 +21,7 @@
 // R * 16 bytes apart (leading byte offset).
 //
 // A CTA walks tiles of 128 particles (the launch gives one tile per CTA);
-// it allocates its tensor memory (32 columns), initialises its mbarrier and
+// it allocates its tensor memory (32 columns, 64 for order 4), initialises its mbarrier and
 // stages W once. The wait on the MMA's mbarrier is bounded; when it runs out the kernel
 // records PRT_ERR_TIMEOUT, skips the update and the remaining tiles, waits
 // again (bounded) and frees its tensor memory.
@@ -29,6 +29,7 @@
 #include <cuda_bf16.h>
 
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "push.cuh"
@@ -44,11 +45,14 @@ struct MixedShape {
   static constexpr int NP = Lagrange<ORDER>::NP;
   static constexpr int KP = (NP + 15) / 16 * 16;    // monomials, padded to the K step (16)
   static constexpr int NPAD = (NP + 15) / 16 * 16;  // Lagrange values (N % 16 == 0 at M = 128)
-  static constexpr int COLS = 32;                   // tensor-memory columns (>= NPAD)
+  // tensor-memory columns: a power of two >= 32 and >= NPAD
+  static constexpr int COLS = NPAD <= 32 ? 32 : 64;
   static constexpr int A_BYTES = MX_BLOCK * KP * 2; // one BF16 term of the monomials
   static constexpr int B_BYTES = NPAD * KP * 2;     // one BF16 term of W
   static constexpr int SMEM = 3 * A_BYTES + 3 * B_BYTES + 16;
-  static_assert(NPAD <= COLS, "mixed stage: orders 1-3");
+  // Lagrange values read back per thread: 32 columns, plus 8 more for order 4
+  static constexpr int LV = NP > 32 ? 40 : 32;
+  static_assert(NPAD <= COLS && NP <= LV, "mixed stage: orders 1-4");
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -235,8 +239,8 @@ __global__ void __launch_bounds__(MX_BLOCK)
     const bool done = mbar_wait_bounded(bar_a, parity);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     ok = __syncthreads_and(done) != 0;  // CTA-uniform: every thread leaves together
-    // this warp's 32 lanes, 32 columns: row = particle
-    uint32_t lv[32];
+    // this warp's 32 lanes, 32 (40) columns: row = particle
+    uint32_t lv[SH::LV];
     if (ok) {
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -251,6 +255,14 @@ __global__ void __launch_bounds__(MX_BLOCK)
             "=r"(lv[27]), "=r"(lv[28]), "=r"(lv[29]), "=r"(lv[30]), "=r"(lv[31])
           : "r"(tmem + ((uint32_t)(warp * 32) << 16))
           : "memory");
+      if constexpr (SH::LV > 32) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+            : "=r"(lv[32]), "=r"(lv[33]), "=r"(lv[34]), "=r"(lv[35]), "=r"(lv[36]),
+              "=r"(lv[37]), "=r"(lv[38]), "=r"(lv[39])
+            : "r"(tmem + ((uint32_t)(warp * 32) << 16) + 32u)
+            : "memory");
+      }
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
     } else {
       if (live) record_error(st, PRT_ERR_TIMEOUT, i);
@@ -338,7 +350,18 @@ int launch(const prt_pusher *P, prt_workspace *ws, long long n, double *x, doubl
            const double *q, const double *m, uint32_t *el, double *kx, double *kp,
            const Fields6 &F, double a, double b, double dt, double c, cudaStream_t s) {
   using SH = MixedShape<ORDER>;
-  static_assert(SH::SMEM <= 48 * 1024, "mixed stage shared memory within the default limit");
+  static_assert(SH::SMEM <= 227 * 1024, "mixed stage shared memory within a CTA's limit");
+  if constexpr (SH::SMEM > 48 * 1024) {
+    // order 4: above the default dynamic shared-memory limit (once per process;
+    // the attribute holds for every device the kernel runs on)
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+      attr = cudaFuncSetAttribute(lsrk_stage_mixed_kernel<ORDER>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SH::SMEM);
+    });
+    PRT_CHECK_CUDA(attr);
+  }
   ScopedTimer timer(ws, PRT_TIME_LSRK_STAGE, s);
   // one CTA per tile of 128 particles measured fastest (2.36 ms per 16M-particle
   // stage on B200, against 2.4-3.7 ms with 3-7 CTAs per SM walking the tiles):
@@ -359,8 +382,9 @@ int prt_pusher_prepare_mixed(prt_pusher *P) {
     case 1: return prepare<1>(P);
     case 2: return prepare<2>(P);
     case 3: return prepare<3>(P);
+    case 4: return prepare<4>(P);
   }
-  return PRT_OK;  // order 4: FP64 stage only
+  return PRT_OK;
 }
 
 int launch_stage_mixed(const prt_pusher *P, prt_workspace *ws, long long n, double *x,
@@ -371,6 +395,7 @@ int launch_stage_mixed(const prt_pusher *P, prt_workspace *ws, long long n, doub
     case 1: return launch<1>(P, ws, n, x, p, q, m, el, kx, kp, F, a, b, dt, c, s);
     case 2: return launch<2>(P, ws, n, x, p, q, m, el, kx, kp, F, a, b, dt, c, s);
     case 3: return launch<3>(P, ws, n, x, p, q, m, el, kx, kp, F, a, b, dt, c, s);
+    case 4: return launch<4>(P, ws, n, x, p, q, m, el, kx, kp, F, a, b, dt, c, s);
   }
   return PRT_ERR_INVALID_ARGUMENT;
 }
