@@ -668,7 +668,7 @@ def main():
                                    f"{w.shape_radius * 100:g} cm, chosen (mixed) form",
                        "particles_per_gpu": n, "elements": w.mesh.element_count,
                        "nodes": nn, "order": w.order, "form": "mixed",
-                       "l2": "inputs larger than L2 (3.5 GB particle state per stage)",
+                       "l2": f"inputs larger than L2 ({216 * n / 1e9:.1f} GB particle state per stage)",
                        "parallelism": f"particles sharded over {world} GPU(s), NCCL "
                                       "all-reduce of rho/j" if world > 1 else "1 GPU"},
             "clocks": clk, "gpu_launches": None, "roofline": roofline,
