@@ -23,6 +23,7 @@ import torch
 
 from . import _lib
 from .meshdata import MeshData
+from .tools import StatePassingNumberShiftMultiplexer, compaction_moves
 
 # Carpenter & Kennedy (1994), 5-stage 4th-order 2N-storage Runge-Kutta: the
 # LSRK4 stepper the reference drives its particles with (driver.py:53,108).
@@ -119,8 +120,12 @@ class PicState:
     stable ids [n]; LSRK residuals kx, kp [3, n]."""
 
     def __init__(self, method, x=None, p=None, q=None, m=None, el=None, ids=None,
-                 depositor_state=None, pusher_state=None, vis_listener=None):
+                 depositor_state=None, pusher_state=None, vis_listener=None, pnss=None):
         self.method = method
+        # particle numbers are ranks in ascending id order (the host views'
+        # order); kills shift them (cloud.py:75-84)
+        self.particle_number_shift_signaller = (
+            StatePassingNumberShiftMultiplexer(self) if pnss is None else pnss)
         dev = device()
         if x is None:
             x = torch.empty((3, 0), dtype=F64, device=dev)
@@ -238,7 +243,10 @@ class PicMethod:
         return "%dd%dv" % (self.dimensions_pos, self.dimensions_velocity)
 
     def make_state(self) -> PicState:
-        return PicState(self)
+        state = PicState(self)
+        state.particle_number_shift_signaller.subscribe_with_state(self.depositor)
+        state.particle_number_shift_signaller.subscribe_with_state(self.pusher)
+        return state
 
     # --- status ------------------------------------------------------------
     def check_status(self, clear=True):
@@ -330,6 +338,7 @@ class PicMethod:
         state.ids = torch.cat([state.ids, ids]).contiguous()
         state.kx = state.kp = None
         self.check_containment(state)
+        state.particle_number_shift_signaller.note_change_size(len(state))
         state.derived_quantity_cache.clear()
 
     def check_containment(self, state):
@@ -346,6 +355,9 @@ class PicMethod:
         alive = state.el != -1
         dead = int((~alive).sum().item())
         if dead:
+            # the shifts of the particle numbers (ranks in id order)
+            order = state.id_order()
+            moves = compaction_moves(alive[order].cpu().numpy().tolist())
             state.x = state.x[:, alive].contiguous()
             state.p = state.p[:, alive].contiguous()
             state.q = state.q[alive].contiguous()
@@ -356,6 +368,10 @@ class PicMethod:
                 state.kx = state.kx[:, alive].contiguous()
                 state.kp = state.kp[:, alive].contiguous()
             state.derived_quantity_cache.clear()
+            sig = state.particle_number_shift_signaller
+            for orig, dest, size in moves:
+                sig.note_move(orig, dest, size)
+            sig.note_change_size(len(state))
         return dead
 
     # --- kinematics --------------------------------------------------------
@@ -411,7 +427,8 @@ class PicMethod:
         new = PicState(self, x=x, p=p, q=state.q, m=state.m, el=state.el.clone(),
                        ids=state.ids, depositor_state=self.depositor.advance_state(state, ddep),
                        pusher_state=self.pusher.advance_state(state),
-                       vis_listener=state.vis_listener)
+                       vis_listener=state.vis_listener,
+                       pnss=state.particle_number_shift_signaller)
         new.next_id = state.next_id
         _lib.check(self.lib.prt_update_containing_elements(
             self.mesh_data.handle, self.workspace, len(new), new.x.data_ptr(),

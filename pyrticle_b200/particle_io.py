@@ -49,6 +49,9 @@ def load_checkpoint(method, path):
         tid = torch.as_tensor(ids, dtype=torch.int64, device=dev)
         state = PicState(method, x=x, p=p, q=q, m=m, el=el, ids=tid)
         state.next_id = max(int(f["next_id"]), state.next_id)
+    state.particle_number_shift_signaller.subscribe_with_state(method.depositor)
+    state.particle_number_shift_signaller.subscribe_with_state(method.pusher)
+    state.particle_number_shift_signaller.note_change_size(len(state))
     return state
 
 

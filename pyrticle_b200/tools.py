@@ -141,3 +141,82 @@ class WarningIgnorer:
 
 
 warning_forwarder = WarningForwarder()
+
+
+# particle-number shifts -------------------------------------------------------
+class NumberShiftMultiplexer:
+    """Fans particle-number shifts out to its subscribers (the reference's
+    tools.py:52-73): note_change_size(new_size), note_move(orig, dest, size)
+    (particles [orig, orig + size) now live at [dest, dest + size)) and
+    note_reset(start, size). Subscribers are held weakly."""
+
+    def __init__(self, name=None):
+        import weakref
+        self.subscribers = weakref.WeakKeyDictionary()
+        self.name = name
+
+    def subscribe(self, subscriber):
+        self.subscribers[subscriber] = None
+
+    def note_change_size(self, new_size):
+        for s in list(self.subscribers.keys()):
+            s.note_change_size(new_size)
+
+    def note_move(self, orig, dest, size):
+        for s in list(self.subscribers.keys()):
+            s.note_move(orig, dest, size)
+
+    def note_reset(self, start, size):
+        for s in list(self.subscribers.keys()):
+            s.note_reset(start, size)
+
+
+class StatePassingNumberShiftMultiplexer(NumberShiftMultiplexer):
+    """Also notifies subscribers that take the particle state as their first
+    argument (depositors and pushers; tools.py:78-103)."""
+
+    def __init__(self, state):
+        import weakref
+        NumberShiftMultiplexer.__init__(self)
+        self.subscribers_with_state = weakref.WeakKeyDictionary()
+        self.state = state
+
+    def subscribe_with_state(self, subscriber):
+        self.subscribers_with_state[subscriber] = None
+
+    def note_change_size(self, new_size):
+        NumberShiftMultiplexer.note_change_size(self, new_size)
+        for s in list(self.subscribers_with_state.keys()):
+            s.note_change_size(self.state, new_size)
+
+    def note_move(self, orig, dest, size):
+        NumberShiftMultiplexer.note_move(self, orig, dest, size)
+        for s in list(self.subscribers_with_state.keys()):
+            s.note_move(self.state, orig, dest, size)
+
+    def note_reset(self, start, size):
+        NumberShiftMultiplexer.note_reset(self, start, size)
+        for s in list(self.subscribers_with_state.keys()):
+            s.note_reset(self.state, start, size)
+
+
+def compaction_moves(alive):
+    """The note_move calls that turn a store into its survivors, keeping their
+    order: runs of surviving particles, (orig, dest, size) with dest <= orig,
+    to be applied in the order given. `alive`: boolean sequence."""
+    moves = []
+    dest = 0
+    i = 0
+    n = len(alive)
+    while i < n:
+        if not alive[i]:
+            i += 1
+            continue
+        j = i
+        while j < n and alive[j]:
+            j += 1
+        if dest != i:
+            moves.append((i, dest, j - i))
+        dest += j - i
+        i = j
+    return moves

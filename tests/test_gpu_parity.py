@@ -97,7 +97,27 @@ def test_relocation_bitexact_with_counters_and_kills(setup):
     dp = np.zeros_like(dx)
     before = (m.find_same_counter, m.find_by_neighbor_counter, m.find_by_vertex_counter,
               m.find_global_counter)
+
+    class ShiftRecorder:
+        """A per-particle array kept in step through the number shifts."""
+
+        def __init__(self, ids):
+            self.ids = list(ids)
+
+        def note_move(self, orig, dest, size):
+            self.ids[dest:dest + size] = self.ids[orig:orig + size]
+
+        def note_change_size(self, n):
+            del self.ids[n:]
+
+        def note_reset(self, start, size):
+            pass
+
+    rec = ShiftRecorder(s.particle_ids)
+    s.particle_number_shift_signaller.subscribe(rec)
     new = m.advance_state(s, dx, dp, None)
+    # the kills reached the subscribers as moves + a size change (id order)
+    assert rec.ids == list(new.particle_ids)
     got = (m.find_same_counter - before[0], m.find_by_neighbor_counter - before[1],
            m.find_by_vertex_counter - before[2], m.find_global_counter - before[3])
     r = O.update_containing_elements(om, w.positions + dx, w.momenta, w.charges, w.masses, el0)

@@ -108,3 +108,51 @@ def test_workload_generators_are_seeded():
     assert np.array_equal(a.positions, b.positions) and np.array_equal(a.fields, b.fields)
     r = np.hypot(a.positions[:, 0] - 0.005, a.positions[:, 1] - 0.005)
     assert r.max() < 0.0025
+
+
+def test_number_shift_multiplexers():
+    """Fan-out of particle-number shifts (tools.py:52-103 of the reference)
+    and the moves of an order-keeping compaction."""
+    from pyrticle_b200.tools import (NumberShiftMultiplexer, StatePassingNumberShiftMultiplexer,
+                                     compaction_moves)
+
+    class Rec:
+        def __init__(self):
+            self.calls = []
+
+        def note_change_size(self, *a):
+            self.calls.append(("size",) + a)
+
+        def note_move(self, *a):
+            self.calls.append(("move",) + a)
+
+        def note_reset(self, *a):
+            self.calls.append(("reset",) + a)
+
+    state = object()
+    sig = StatePassingNumberShiftMultiplexer(state)
+    plain, with_state = Rec(), Rec()
+    sig.subscribe(plain)
+    sig.subscribe_with_state(with_state)
+    sig.note_move(5, 2, 3)
+    sig.note_change_size(7)
+    sig.note_reset(0, 4)
+    assert plain.calls == [("move", 5, 2, 3), ("size", 7), ("reset", 0, 4)]
+    assert with_state.calls == [("move", state, 5, 2, 3), ("size", state, 7),
+                                ("reset", state, 0, 4)]
+    m = NumberShiftMultiplexer()
+    r = Rec()
+    m.subscribe(r)
+    del r  # held weakly
+    m.note_change_size(3)
+    assert len(m.subscribers) == 0
+
+    rng = np.random.default_rng(4)
+    for n in (0, 1, 7, 100):
+        alive = rng.random(n) < 0.6
+        vals = list(range(n))
+        for orig, dest, size in compaction_moves(alive.tolist()):
+            assert dest <= orig
+            vals[dest:dest + size] = vals[orig:orig + size]
+        kept = int(alive.sum())
+        assert vals[:kept] == [i for i in range(n) if alive[i]]
