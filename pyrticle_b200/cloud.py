@@ -23,7 +23,8 @@ import torch
 
 from . import _lib
 from .meshdata import MeshData
-from .tools import StatePassingNumberShiftMultiplexer, compaction_moves
+from .tools import (NumberShiftableVector, StatePassingNumberShiftMultiplexer,
+                    compaction_moves)
 
 # Carpenter & Kennedy (1994), 5-stage 4th-order 2N-storage Runge-Kutta: the
 # LSRK4 stepper the reference drives its particles with (driver.py:53,108).
@@ -504,7 +505,69 @@ class TimesteppablePicState:
         if isinstance(update, (int, float)) and update == 0:
             return self
         dx, dp, ddep = update
+        dx = NumberShiftableVector.unwrap(dx)
+        dp = NumberShiftableVector.unwrap(dp)
+        if isinstance(dx, (int, float)) and dx == 0:
+            dx = np.zeros((len(self.state), 3))
+        if isinstance(dp, (int, float)) and dp == 0:
+            dp = np.zeros((len(self.state), 3))
         return TimesteppablePicState(self.method,
                                      self.method.advance_state(self.state, dx, dp, ddep))
 
     __radd__ = __add__
+
+
+def _obj_array(items):
+    out = np.empty(len(items), dtype=object)
+    for k, v in enumerate(items):
+        out[k] = v
+    return out
+
+
+class FieldToParticleRhsCalculator:
+    """The particles' momentum right-hand side from the fields (cloud.py:238-290):
+    the pusher's forces at the particles as a number-shiftable vector, in the
+    (dx, dp, ddep) layout of a TimesteppablePicState update.
+
+    ``maxwell_op`` supplies ``split_eh(fields) -> (e, h)``, ``get_eh_subset()``
+    (six flags: which of ex, ey, ez, hx, hy, hz the field vector carries) and
+    ``mu`` (B = mu H); absent components are zero."""
+
+    def __init__(self, method, maxwell_op):
+        self.method = method
+        self.maxwell_op = maxwell_op
+
+    def __call__(self, t, fields_f, state_f):
+        fields = fields_f()
+        state = state_f()
+        e, h = self.maxwell_op.split_eh(fields)
+        subset = list(self.maxwell_op.get_eh_subset())
+        e_arg, b_arg = [], []
+        idx = 0
+        for use in subset[0:3]:
+            e_arg.append(e[idx] if use else None)
+            idx += 1 if use else 0
+        idx = 0
+        for use in subset[3:6]:
+            b_arg.append(self.maxwell_op.mu * h[idx] if use else None)
+            idx += 1 if use else 0
+        velocities = self.method.velocities(state)
+        forces = self.method.pusher.forces(state, velocities, *(e_arg + b_arg))
+        return _obj_array([0, NumberShiftableVector(
+            forces, signaller=state.particle_number_shift_signaller), 0])
+
+
+class ParticleRhsCalculator:
+    """The particles' position right-hand side (cloud.py:293-311): their
+    velocities as a number-shiftable vector, plus the depositor's rhs."""
+
+    def __init__(self, method, maxwell_op=None):
+        self.method = method
+        self.maxwell_op = maxwell_op
+
+    def __call__(self, t, fields_f, state_f):
+        state = state_f()
+        velocities = self.method.velocities(state)
+        return _obj_array([NumberShiftableVector(
+            velocities, signaller=state.particle_number_shift_signaller), 0,
+            self.method.depositor.rhs(state)])

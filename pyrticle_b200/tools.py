@@ -220,3 +220,51 @@ def compaction_moves(alive):
         dest += j - i
         i = j
     return moves
+
+
+class NumberShiftableVector:
+    """A per-particle host vector (rows = particle numbers) kept in step with
+    the particle-number shifts of its signaller (tools.py:106-177), so that
+    RK stage vectors survive particles being removed in mid-step. Adds and
+    scales like its vector; `unwrap` returns the plain vector."""
+
+    def __init__(self, vector, signaller):
+        self.vector = vector
+        self.signaller = signaller
+        signaller.subscribe(self)
+
+    @staticmethod
+    def unwrap(instance):
+        return instance.vector if isinstance(instance, NumberShiftableVector) else instance
+
+    def __len__(self):
+        return len(self.vector)
+
+    def __add__(self, other):
+        return NumberShiftableVector(self.vector + self.unwrap(other), self.signaller)
+
+    __radd__ = __add__
+
+    def __iadd__(self, other):
+        self.vector += self.unwrap(other)
+        return self
+
+    def __mul__(self, other):
+        return NumberShiftableVector(self.vector * self.unwrap(other), self.signaller)
+
+    __rmul__ = __mul__
+
+    def note_change_size(self, new_size):
+        old = len(self.vector)
+        if new_size > old:
+            grown = np.zeros((new_size,) + tuple(self.vector.shape[1:]), dtype=self.vector.dtype)
+            grown[:old] = self.vector
+            self.vector = grown
+        elif new_size < old:
+            self.vector = self.vector[:new_size]
+
+    def note_move(self, orig, dest, size):
+        self.vector[dest:dest + size] = self.vector[orig:orig + size].copy()
+
+    def note_reset(self, start, size):
+        self.vector[start:start + size] = 0

@@ -156,3 +156,23 @@ def test_number_shift_multiplexers():
             vals[dest:dest + size] = vals[orig:orig + size]
         kept = int(alive.sum())
         assert vals[:kept] == [i for i in range(n) if alive[i]]
+
+
+def test_number_shiftable_vector():
+    """RK stage vectors follow particle removals (tools.py:106-177)."""
+    from pyrticle_b200.tools import NumberShiftableVector, StatePassingNumberShiftMultiplexer
+    sig = StatePassingNumberShiftMultiplexer(object())
+    v = NumberShiftableVector(np.arange(12.0).reshape(6, 2), sig)
+    w = 2 * v + v
+    assert isinstance(w, NumberShiftableVector)
+    assert np.array_equal(w.vector, 3 * np.arange(12.0).reshape(6, 2))
+    # particles 1 and 4 removed: runs [2, 4) -> 1, [5, 6) -> 3
+    sig.note_move(2, 1, 2)
+    sig.note_move(5, 3, 1)
+    sig.note_change_size(4)
+    keep = [0, 2, 3, 5]
+    assert np.array_equal(v.vector, np.arange(12.0).reshape(6, 2)[keep])
+    assert np.array_equal(w.vector, 3 * np.arange(12.0).reshape(6, 2)[keep])
+    sig.note_change_size(5)
+    assert np.array_equal(v.vector[4], [0, 0])
+    assert NumberShiftableVector.unwrap(v) is v.vector and NumberShiftableVector.unwrap(3) == 3
