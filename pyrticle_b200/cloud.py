@@ -188,10 +188,17 @@ class PicState:
         return self.kx, self.kp
 
     def clear(self):
-        dev = self.x.device
         self.__init__(self.method, depositor_state=self.depositor_state,
-                      pusher_state=self.pusher_state)
+                      pusher_state=self.pusher_state, vis_listener=self.vis_listener,
+                      pnss=self.particle_number_shift_signaller)
         self.derived_quantity_cache.clear()
+        self.particle_number_shift_signaller.note_change_size(0)
+
+    def resize(self, newsize):
+        """Capacity hint (cloud.py:114-124): the device store grows as particles
+        are added, so only a size below the particle count is an error."""
+        if newsize < len(self):
+            raise ValueError("cannot resize below the particle count (%d)" % len(self))
 
     # --- derived quantity cache (cloud.py:133-154) -------------------------
     def get_derived_quantity_from_cache(self, name, getter):
@@ -200,6 +207,21 @@ class PicState:
         except KeyError:
             self.derived_quantity_cache[name] = value = getter()
             return value
+
+    def get_derived_quantities_from_cache(self, names, getters, all_getter=None):
+        """Cached values of several quantities; `all_getter` computes all of
+        them at once when none is cached, else each missing one comes from its
+        getter (which stores it)."""
+        cached = tuple(self.derived_quantity_cache.get(name) for name in names)
+        cached_number = sum(1 for v in cached if v is not None)
+        if cached_number == len(names):
+            return cached
+        if cached_number == 0 and all_getter is not None:
+            values = all_getter()
+            for name, value in zip(names, values):
+                self.derived_quantity_cache[name] = value
+            return tuple(values)
+        return tuple(c if c is not None else g() for c, g in zip(cached, getters))
 
 
 class PicMethod:
@@ -242,6 +264,33 @@ class PicMethod:
 
     def get_dimensionality_suffix(self) -> str:
         return "%dd%dv" % (self.dimensions_pos, self.dimensions_velocity)
+
+    def get_shape_function_class(self):
+        """The shape function the deposition kernels evaluate (cloud.py:391-404):
+        the polynomial one."""
+        from .tools import PolynomialShapeFunction
+        return PolynomialShapeFunction
+
+    def set_ignore_core_warnings(self, ignore):
+        """Forward (False) or drop (True) the library's warnings (cloud.py:406-413)."""
+        from . import tools
+        tools.warning_forwarder = tools.WarningIgnorer() if ignore else tools.WarningForwarder()
+
+    def add_instrumentation(self, mgr, observer):
+        """Log quantities of the element finder and of the depositor and pusher
+        (cloud.py:415-423): the four find counters, as events per tick."""
+        from .log import FindCounter
+        for attr, name, desc in (
+                ("find_same_counter", "n_find_same", "#Particles found in same element"),
+                ("find_by_neighbor_counter", "n_find_neighbor",
+                 "#Particles found through neighbor"),
+                ("find_by_vertex_counter", "n_find_by_vertex",
+                 "#Particles found by vertex"),
+                ("find_global_counter", "n_find_global", "#Particles found by global search")):
+            mgr.add_quantity(FindCounter(self, attr, name, desc))
+        for part in (self.depositor, self.pusher):
+            if hasattr(part, "add_instrumentation"):
+                part.add_instrumentation(mgr, observer)
 
     def make_state(self) -> PicState:
         state = PicState(self)

@@ -25,6 +25,14 @@ class Depositor:
     def set_shape_function(self, state, sf):
         self.shape_function = sf
 
+    def add_instrumentation(self, mgr, observer):
+        """Log constants: the depositor's class and its parameters
+        (deposition/__init__.py:41-45)."""
+        if hasattr(mgr, "set_constant"):
+            mgr.set_constant("depositor", self.__class__.__name__)
+            for key, value in self.log_constants.items():
+                mgr.set_constant(key, value)
+
     def deposit_hook(self):
         if self.shape_function is None:
             raise RuntimeError("shape function never set")

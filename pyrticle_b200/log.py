@@ -116,6 +116,22 @@ class ParticleCurrent(_Quantity):
                             self.direction))
 
 
+class FindCounter(_Quantity):
+    """Particles located by one branch of the element finder since the last
+    reading (the reference's EventCounter quantities, cloud.py:340-378)."""
+
+    def __init__(self, method, attr, name, description):
+        super().__init__(name, "1", description)
+        self.method = method
+        self.attr = attr
+        self.last = getattr(method, attr)
+
+    def __call__(self):
+        now = getattr(self.method, self.attr)
+        value, self.last = now - self.last, now
+        return value
+
+
 def add_particle_quantities(mgr, observer):
     mgr.add_quantity(ParticleCount(observer))
     mgr.add_quantity(ParticleMomentum(observer))

@@ -28,6 +28,11 @@ class Pusher:
     def upkeep(self, state):
         pass
 
+    def add_instrumentation(self, mgr, observer):
+        """Log constant: the pusher's class (pusher.py:54-57)."""
+        if hasattr(mgr, "set_constant"):
+            mgr.set_constant("pusher", self.__class__.__name__)
+
     def note_move(self, state, orig, dest, size):
         pass
 

@@ -176,3 +176,48 @@ def test_number_shiftable_vector():
     sig.note_change_size(5)
     assert np.array_equal(v.vector[4], [0, 0])
     assert NumberShiftableVector.unwrap(v) is v.vector and NumberShiftableVector.unwrap(3) == 3
+
+
+def test_derived_quantities_cache():
+    """get_derived_quantities_from_cache (cloud.py:141-154) without the
+    reference's always-true count: all cached, none cached (one joint
+    computation), some cached (the missing ones alone)."""
+    from pyrticle_b200.cloud import PicState
+
+    class S:
+        def __init__(self):
+            self.derived_quantity_cache = {}
+
+    s = S()
+    calls = []
+
+    def g(name, val):
+        def f():
+            calls.append(name)
+            s.derived_quantity_cache[name] = val
+            return val
+        return f
+
+    get = PicState.get_derived_quantities_from_cache
+    names = ("a", "b")
+    r = get(s, names, (g("a", 1), g("b", 2)), all_getter=lambda: (calls.append("all") or (1, 2)))
+    assert r == (1, 2) and calls == ["all"] and s.derived_quantity_cache == {"a": 1, "b": 2}
+    del s.derived_quantity_cache["b"]
+    calls.clear()
+    assert get(s, names, (g("a", 1), g("b", 2)), all_getter=None) == (1, 2)
+    assert calls == ["b"]
+    calls.clear()
+    assert get(s, names, (g("a", 1), g("b", 2))) == (1, 2) and calls == []
+
+
+def test_find_counter_log_quantity():
+    from pyrticle_b200.log import FindCounter
+
+    class M:
+        find_same_counter = 5
+
+    m = M()
+    q = FindCounter(m, "find_same_counter", "n_find_same", "d")
+    m.find_same_counter = 12
+    assert q() == 7
+    assert q() == 0

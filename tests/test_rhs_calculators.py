@@ -99,3 +99,54 @@ def test_rk_residuals_follow_removals():
     assert len(out2) == len(out)
     assert rel_l2(out.positions, out2.positions) < 1e-13
     assert rel_l2(out.momenta, out2.momenta) < 1e-13
+
+
+def test_state_helpers_and_instrumentation():
+    w = problems.make("config0", scale=0.02)
+    m = PicMethod(Discretization(w.mesh, w.order, nodes=w.nodes), U, ShapeFunctionDepositor(),
+                  MonomialParticlePusher(), 3, 3)
+
+    class Mgr:
+        def __init__(self):
+            self.quantities, self.constants = [], {}
+
+        def add_quantity(self, q):
+            self.quantities.append(q)
+
+        def set_constant(self, k, v):
+            self.constants[k] = v
+
+    mgr = Mgr()
+    m.add_instrumentation(mgr, None)
+    assert mgr.constants == {"depositor": "ShapeFunctionDepositor",
+                             "pusher": "MonomialParticlePusher"}
+    s = m.make_state()
+    sizes = []
+
+    class Rec:
+        def note_change_size(self, n):
+            sizes.append(n)
+
+        def note_move(self, *a):
+            pass
+
+        def note_reset(self, *a):
+            pass
+
+    rec = Rec()
+    s.particle_number_shift_signaller.subscribe(rec)
+    m.add_particles_from_arrays(s, w.positions, w.momenta, w.charges, w.masses)
+    n = len(s)
+    assert sizes == [n]
+    dx = np.zeros((n, 3))
+    dx[:, 2] = 0.3 * w.shape_radius  # moves into neighbouring elements
+    s = m.advance_state(s, dx, np.zeros((n, 3)), None)
+    found = {q.name: q() for q in mgr.quantities}
+    assert sum(found.values()) == n and found["n_find_global"] >= 0
+    assert all(q() == 0 for q in mgr.quantities)  # events since the last reading
+    with pytest.raises(ValueError):
+        s.resize(n - 1)
+    s.resize(2 * n)
+    s.clear()
+    assert len(s) == 0 and sizes[-1] == 0
+    assert m.get_shape_function_class().__name__ == "PolynomialShapeFunction"
