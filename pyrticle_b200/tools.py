@@ -58,6 +58,43 @@ class PolynomialShapeFunction:
         return "polynomial"
 
 
+class CInfinityShapeFunction:
+    """S(r) = N exp(-1 / (r^2/a^2 - 1)^2) for r <= a, else 0 (tools.hpp:561-591),
+    with N = 1 / (|S^{n-1}| a^n I), I = int_0^1 s^(n-1) exp(-1/(1 - s^2)^2) ds
+    by 50-point Gauss-Legendre on [0, 1] (tools.cpp:63-72, tools.py:268-283).
+    Host evaluation only: the deposition kernels use the polynomial shape,
+    as the reference's compiled depositors do."""
+
+    def __init__(self, radius: float = 1.0, dimensions: int = 1):
+        self.radius = float(radius)
+        self.dimensions = int(dimensions)
+        x, w = np.polynomial.legendre.leggauss(50)
+        s = 0.5 * (x + 1)
+        integral = float(0.5 * np.sum(w * s ** (dimensions - 1)
+                                      * np.exp(-1 / (1 - s ** 2) ** 2)))
+        self.normalizer = 1 / (sphere_area(float(dimensions)) * self.radius ** dimensions
+                               * integral)
+
+    def __call__(self, r) -> float:
+        r = np.asarray(r, dtype=np.float64)
+        r2 = float(np.dot(r, r))
+        if r2 >= self.radius ** 2:  # exp(-1/0) = 0 at the radius itself
+            return 0.0
+        t = r2 / self.radius ** 2 - 1
+        return self.normalizer * math.exp(-1 / (t * t))
+
+    def evaluate(self, r: np.ndarray) -> np.ndarray:
+        """Vectorised over the last axis of ``r``."""
+        r2 = np.sum(np.asarray(r) ** 2, axis=-1)
+        inside = r2 < self.radius ** 2
+        t = np.where(inside, r2 / self.radius ** 2 - 1, -1.0)
+        return np.where(inside, self.normalizer * np.exp(-1 / (t * t)), 0.0)
+
+    @staticmethod
+    def name() -> str:
+        return "c_infinity"
+
+
 class StatsGatherer:
     """Welford mean/variance with min and max (tools.hpp:340-417)."""
 

@@ -85,6 +85,21 @@ def test_shape_function_integrates_to_one(alpha):
     assert abs(integral - 1) < 4e-5
 
 
+def test_c_infinity_shape_function_integrates_to_one():
+    """test_pyrticle.py:389-420 for the C-infinity shape, same mesh and bound."""
+    from pyrticle_b200.tools import CInfinityShapeFunction
+    r = 0.1
+    mesh = meshgen.box_mesh((14, 14, 14), (-r, -r, -r), (r, r, r), jitter=0.0)
+    nodes = meshgen.element_nodes(mesh, 3)
+    sf = CInfinityShapeFunction(r, 3)
+    vals = sf.evaluate(nodes)
+    w = refelement.integration_weights(3)
+    integral = float((vals.reshape(-1, len(w)) @ w * mesh.jacobians).sum())
+    assert abs(integral - 1) < 4e-5
+    assert sf(np.zeros(3)) == pytest.approx(sf.normalizer * math.exp(-1))
+    assert sf(np.array([r, 0, 0])) == 0.0
+
+
 def test_global_search_bins_equal_linear_scan(small_workload, oracle_mesh):
     w = small_workload
     rng = np.random.default_rng(5)
