@@ -620,3 +620,53 @@ class ParticleRhsCalculator:
         return _obj_array([NumberShiftableVector(
             velocities, signaller=state.particle_number_shift_signaller), 0,
             self.method.depositor.rhs(state)])
+
+
+# shape bandwidth --------------------------------------------------------------
+def guess_shape_bandwidth(method, state, exponent):
+    """Shape radius from the mesh (cloud.py:680-686): the mesh data's
+    advisable particle radius."""
+    method.depositor.set_shape_function(state, method.get_shape_function_class()(
+        method.mesh_data.advisable_particle_radius(), method.mesh_data.dimensions, exponent))
+
+
+def optimize_shape_bandwidth(method, state, analytic_rho, exponent):
+    """Shape radius that best reproduces `analytic_rho` (cloud.py:691-824):
+    50 radii from 2^-4 to 2^2 times the advisable one (log-spaced), each
+    deposition's L1 error against `analytic_rho`; the largest radius at a
+    local minimum of the error is set (a warning when even the best relative
+    L1 error exceeds 0.1). Returns (chosen radius, tried radii, L1 errors)."""
+    discr = method.discretization
+    adv = method.mesh_data.advisable_particle_radius()
+    radii = [adv * 2 ** i for i in np.linspace(-4, 2, 50)]
+    cls = method.get_shape_function_class()
+
+    def set_radius(r):
+        method.depositor.set_shape_function(state, cls(r, method.mesh_data.dimensions, exponent))
+
+    tried, errors = [], []
+    for radius in radii:
+        try:
+            method.set_ignore_core_warnings(True)
+            set_radius(radius)
+            state.derived_quantity_cache.clear()
+            rec_rho = method.deposit_rho(state)
+        except RuntimeError as exc:
+            if "particle mass is zero" in str(exc):
+                continue
+            raise
+        finally:
+            method.set_ignore_core_warnings(False)
+        tried.append(radius)
+        errors.append(discr.integral(np.abs(rec_rho - analytic_rho)))
+    best = int(np.argmin(errors))
+    rel = abs(errors[best] / discr.integral(analytic_rho))
+    if rel > 0.1:
+        import warnings
+        warnings.warn("Charge density is very poorly resolved (rel L1 error=%g)" % rel)
+    minima = [i for i in range(1, len(errors) - 1)
+              if errors[i] < errors[i - 1] and errors[i] < errors[i + 1]]
+    chosen = tried[max(minima)] if minima else tried[best]
+    set_radius(chosen)
+    state.derived_quantity_cache.clear()
+    return chosen, tried, errors

@@ -150,3 +150,28 @@ def test_state_helpers_and_instrumentation():
     s.clear()
     assert len(s) == 0 and sizes[-1] == 0
     assert m.get_shape_function_class().__name__ == "PolynomialShapeFunction"
+
+
+def test_shape_bandwidth_helpers():
+    """guess_shape_bandwidth and optimize_shape_bandwidth (cloud.py:680-824)
+    on the config0 beam (uniform in a cylinder of radius 0.25 cm over
+    z in [0.5, 3.5] cm) against its analytic charge density."""
+    from pyrticle_b200.cloud import guess_shape_bandwidth, optimize_shape_bandwidth
+    w = problems.make("config0", scale=1.0)
+    m = PicMethod(Discretization(w.mesh, w.order, nodes=w.nodes), U, ShapeFunctionDepositor(),
+                  MonomialParticlePusher(), 3, 3)
+    s = m.make_state()
+    m.add_particles_from_arrays(s, w.positions, w.momenta, w.charges, w.masses)
+    guess_shape_bandwidth(m, s, 2)
+    assert m.depositor.shape_function.radius == m.mesh_data.advisable_particle_radius()
+    CM = 1e-2
+    nodes = np.asarray(m.discretization.nodes)
+    r2 = (nodes[:, 0] - 0.5 * CM) ** 2 + (nodes[:, 1] - 0.5 * CM) ** 2
+    inside = (r2 < (0.25 * CM) ** 2) & (nodes[:, 2] > 0.5 * CM) & (nodes[:, 2] < 3.5 * CM)
+    rho0 = float(np.sum(w.charges)) / (np.pi * (0.25 * CM) ** 2 * 3 * CM)
+    analytic = np.where(inside, rho0, 0.0)
+    chosen, tried, errors = optimize_shape_bandwidth(m, s, analytic, 2)
+    i = tried.index(chosen)
+    assert 0 < i < len(tried) - 1 and errors[i] < errors[i - 1] and errors[i] < errors[i + 1]
+    assert m.depositor.shape_function.radius == chosen
+    assert errors[i] / abs(m.discretization.integral(analytic)) < 0.5
