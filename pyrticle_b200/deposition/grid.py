@@ -293,6 +293,58 @@ def orthonormal_vandermonde_fast(points, modes):
     return refelement.orthonormal_vandermonde(points, modes)
 
 
+def average_groups(mesh, nodes, nodes_per_element, chunk=200000):
+    """The continuity groups of prepare_average_groups (grid.py:143-183): the
+    DG nodes that face pairs identify, merged into connected sets. For every
+    interior face (periodic ones included: positions compared modulo the
+    period) the nodes of both elements lying on it are matched by position;
+    the groups are the connected components of those matches with two or
+    more nodes, each in ascending node order. Returns (starts[G+1], nodes)."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    E, Np = mesh.element_count, nodes_per_element
+    X = nodes.reshape(E, Np, 3)
+    h = float(np.median(mesh.inradii()))
+    tol = 1e-6 * h
+    # [E, 4, Np]: node on face f of its element
+    dist = np.einsum("enk,efk->efn", X, mesh.face_normals) - mesh.face_plane_rhs[:, :, None]
+    on_face = np.abs(dist) <= tol
+    nb = mesh.face_neighbors.astype(np.int64)
+    inval = np.iinfo(np.uint32).max
+    e_idx, f_idx = np.nonzero((nb != inval) & (nb > np.arange(E)[:, None]))
+    per = mesh.periodicity_max - mesh.periodicity_min
+    rows, cols = [], []
+    for c0 in range(0, len(e_idx), chunk):
+        e1 = e_idx[c0:c0 + chunk]
+        f1 = f_idx[c0:c0 + chunk]
+        e2 = nb[e1, f1]
+        # the face of e2 that points back at e1
+        f2 = np.argmax(mesh.face_neighbors[e2].astype(np.int64) == e1[:, None], axis=1)
+        m1 = on_face[e1, f1]                    # [F, Np]
+        m2 = on_face[e2, f2]
+        d = X[e1][:, :, None, :] - X[e2][:, None, :, :]   # [F, Np, Np, 3]
+        for ax in range(3):
+            if per[ax] > 0:
+                d[..., ax] -= np.round(d[..., ax] / per[ax]) * per[ax]
+        close = (np.abs(d).max(axis=-1) <= tol) & m1[:, :, None] & m2[:, None, :]
+        fi, a, b = np.nonzero(close)
+        rows.append(e1[fi] * Np + a)
+        cols.append(e2[fi] * Np + b)
+    rows = np.concatenate(rows) if rows else np.zeros(0, np.int64)
+    cols = np.concatenate(cols) if cols else np.zeros(0, np.int64)
+    nn = E * Np
+    g = coo_matrix((np.ones(len(rows)), (rows, cols)), shape=(nn, nn))
+    ncomp, labels = connected_components(g, directed=False)
+    sizes = np.bincount(labels, minlength=ncomp)
+    member = sizes[labels] >= 2
+    order = np.lexsort((np.arange(nn), labels))     # by group, ascending node inside
+    order = order[member[order]]
+    lab = labels[order]
+    starts = np.concatenate([[0], np.nonzero(np.diff(lab))[0] + 1, [len(order)]])
+    return starts.astype(np.uint32), order.astype(np.uint32)
+
+
 class GridDepositor(Depositor):
     """Deposit on brick grids (shape-function values at the points, or
     trilinear weights with ``grid_weights="trilinear"``), then remap."""
@@ -362,6 +414,13 @@ class GridDepositor(Depositor):
         d.eog_matrix_starts = _lib.ptr(arr(mstarts, np.uint64), C.c_uint64)
         d.eog_matrices = _lib.ptr(arr(mats, np.float64))
         d.avg_group_count = 0
+        if self.enforce_continuity:
+            ag_starts, ag_nodes = average_groups(discr.mesh, np.asarray(discr.nodes),
+                                                 discr.nodes_per_element)
+            self.average_group_starts, self.average_groups = ag_starts, ag_nodes
+            d.avg_group_count = len(ag_starts) - 1
+            d.avg_group_starts = _lib.ptr(arr(ag_starts, np.uint32), C.c_uint32)
+            d.avg_group_nodes = _lib.ptr(arr(ag_nodes, np.uint32), C.c_uint32)
         if self.jiggle_radius:
             d.point_origins = _lib.ptr(arr(np.stack([b.point_origins for b in self.bricks]),
                                            np.float64))

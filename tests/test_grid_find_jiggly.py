@@ -255,3 +255,29 @@ def test_jiggly_grid_gpu_matches_oracle(small_workload, oracle_mesh):
     m2.add_particles_from_arrays(s2, w.positions, w.momenta, w.charges, w.masses)
     gr2, _ = reg.deposit_grid_densities_device(s2)
     assert rel_l2(gr2.cpu().numpy(), gro) > 1e-3
+
+
+@pytest.mark.gpu
+def test_grid_remap_with_continuity_groups(small_workload, oracle_mesh):
+    """GridDepositor(enforce_continuity=True): the averaging groups of
+    prepare_average_groups (grid.py:143-183) applied after the remap, GPU
+    against the oracle's remap (1e-12), and every group single-valued."""
+    PicMethod, GridDepositor, _, Discretization, Pusher = _gpu_imports()
+    w = small_workload
+    dep = GridDepositor(brick_generator=SingleBrickGenerator(dims=(24, 24, 96)),
+                        enforce_continuity=True)
+    meth = PicMethod(Discretization(w.mesh, w.order, nodes=w.nodes), U, dep, Pusher(), 3, 3)
+    sf = PolynomialShapeFunction(w.shape_radius, 3, 2)
+    dep.set_shape_function(None, sf)
+    s = meth.make_state()
+    meth.add_particles_from_arrays(s, w.positions, w.momenta, w.charges, w.masses)
+    gr, _ = dep.deposit_grid_densities_device(s, j=False)
+    rho = dep.remap_grid_to_mesh_device(gr).cpu().numpy()
+    to = np.zeros(len(meth.discretization))
+    O.remap_grid_to_mesh(dep.grid_desc, np.ascontiguousarray(gr.cpu().numpy()), to)
+    assert rel_l2(rho, to) < TOL
+    st, nd = dep.average_group_starts, dep.average_groups
+    assert len(st) > 1000
+    for g in range(0, len(st) - 1, 7):
+        vals = rho[nd[st[g]:st[g + 1]]]
+        assert np.all(vals == vals[0])
