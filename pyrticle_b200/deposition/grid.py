@@ -490,6 +490,20 @@ class GridDepositor(Depositor):
     def deposit_grid_j(self, state, velocities=None, pslice=None):
         return self.deposit_grid_densities_device(state, False, True)[1].T.contiguous().cpu().numpy()
 
+    def deposit_grid_densities(self, state, velocities=None, pslice=None):
+        """(rho_grid [G], j_grid [G, 3]) in one pass (grid.py:820-829)."""
+        gr, gj = self.deposit_grid_densities_device(state, True, True)
+        return gr.cpu().numpy(), gj.T.contiguous().cpu().numpy()
+
+    # grid debug quantities (grid.py:848-858)
+    def ones_on_grid(self):
+        return np.ones((self.grid_node_count_with_extra(),), dtype=float)
+
+    def grid_usecount(self):
+        """How many elements' interpolation uses each grid point."""
+        return np.bincount(np.asarray(self.eog["grid_nodes"], dtype=np.int64),
+                           minlength=self.grid_node_count_with_extra()).astype(float)
+
     def remap_grid_to_mesh(self, q_grid):
         t = torch.as_tensor(np.ascontiguousarray(q_grid), device=self.method.dev)
         if t.dim() == 2:

@@ -281,3 +281,26 @@ def test_grid_remap_with_continuity_groups(small_workload, oracle_mesh):
     for g in range(0, len(st) - 1, 7):
         vals = rho[nd[st[g]:st[g + 1]]]
         assert np.all(vals == vals[0])
+
+
+@pytest.mark.gpu
+def test_grid_host_entry_points(small_workload):
+    """deposit_grid_densities / deposit_grid_rho / deposit_grid_j and the
+    debug quantities (grid.py:820-858) agree with the device entry points."""
+    PicMethod, GridDepositor, _, Discretization, Pusher = _gpu_imports()
+    w = small_workload
+    dep = GridDepositor(brick_generator=SingleBrickGenerator(dims=(24, 24, 96)))
+    meth = PicMethod(Discretization(w.mesh, w.order, nodes=w.nodes), U, dep, Pusher(), 3, 3)
+    dep.set_shape_function(None, PolynomialShapeFunction(w.shape_radius, 3, 2))
+    s = meth.make_state()
+    meth.add_particles_from_arrays(s, w.positions, w.momenta, w.charges, w.masses)
+    gr, gj = dep.deposit_grid_densities(s, meth.velocities(s))
+    assert np.array_equal(gr, dep.deposit_grid_rho(s))
+    assert np.array_equal(gj, dep.deposit_grid_j(s, meth.velocities(s)))
+    assert gj.shape == (dep.grid_node_count, 3)
+    rho = dep.remap_grid_to_mesh(gr)
+    j = dep.remap_grid_to_mesh(gj)
+    assert rho.shape == (len(meth.discretization),) and j.shape == (len(meth.discretization), 3)
+    assert np.array_equal(rho, meth.deposit_rho(s))
+    use = dep.grid_usecount()
+    assert use.sum() == len(dep.eog["grid_nodes"]) and np.all(dep.ones_on_grid() == 1)
