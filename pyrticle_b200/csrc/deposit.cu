@@ -202,6 +202,10 @@ constexpr int WARPS = BLOCK / 32;
 #define PRT_MIXED_UNROLL 2
 #endif
 constexpr int FP64_UNROLL = PRT_FP64_UNROLL;
+// launch the position groups heaviest first (1) or in Morton order (0)
+#ifndef PRT_DEPOSIT_HEAVY_FIRST
+#define PRT_DEPOSIT_HEAVY_FIRST 1
+#endif
 constexpr int MIXED_UNROLL = PRT_MIXED_UNROLL;
 // per-warp ring of compacted particles (two batches of 32)
 constexpr int RING = 64;
@@ -337,6 +341,34 @@ __device__ __forceinline__ void warp_box(const double *__restrict__ pos, uint32_
     }
 }
 
+// Work estimate per position group: the particles in the bin rows of its
+// sphere grown by the radius (periodic images ignored), keyed for a
+// descending sort so that the heaviest groups start first and the light
+// ones fill the tail of the launch. Each group is still walked by one warp,
+// so the order changes no result.
+__global__ void group_work_kernel(long long ngroups, const double *__restrict__ gspheres,
+                                  BinGrid G, const uint32_t *__restrict__ starts,
+                                  double radius, uint32_t *__restrict__ work,
+                                  uint32_t *__restrict__ ids) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  const double r = gspheres[4 * g + 3] + radius;
+  int lo[3], hi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = max(0, min(G.dims[d] - 1, bin_floor(G, d, gspheres[4 * g + d] - r)));
+    hi[d] = max(0, min(G.dims[d] - 1, bin_floor(G, d, gspheres[4 * g + d] + r)));
+  }
+  unsigned long long wsum = 0;
+  for (int bz = lo[2]; bz <= hi[2]; ++bz)
+    for (int by = lo[1]; by <= hi[1]; ++by) {
+      const long long row = (long long)G.dims[0] * (by + (long long)G.dims[1] * bz);
+      wsum += starts[row + hi[0] + 1] - starts[row + lo[0]];
+    }
+  work[g] = (uint32_t)min(wsum, 0xffffffffull);
+  ids[g] = (uint32_t)g;
+}
+
 // One warp per position group (<= 32 positions, one per lane), warps fully
 // independent (no block-level barrier). The warp streams the particles of
 // the bin rows within its sphere grown by the radius straight from L2/L1:
@@ -356,13 +388,15 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
                           const double *__restrict__ gspheres,
                           const uint32_t *__restrict__ run_starts, BinGrid G,
                           DepParticles P, ShapeParams S, long long npos,
-                          double *__restrict__ out, unsigned long long *__restrict__ counters) {
+                          double *__restrict__ out, unsigned long long *__restrict__ counters,
+                          const uint32_t *__restrict__ order = nullptr) {
   // ring entries: (wx, wy), (wz, |w|^2), (q N, q N vx), (q N vy, q N vz)
   __shared__ double2 ring[WARPS][4][RING];
 
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const long long g = blockIdx.x * (long long)WARPS + wid;
-  if (g >= ngroups) return;  // whole warp
+  const long long gi = blockIdx.x * (long long)WARPS + wid;
+  if (gi >= ngroups) return;  // whole warp
+  const long long g = order ? (long long)order[gi] : gi;
   const uint32_t p0 = gstarts[g];
   const int npg = (int)(gstarts[g + 1] - p0);
   double2(*R)[RING] = ring[wid];
@@ -511,7 +545,8 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
                                 const uint32_t *__restrict__ gstarts,
                                 const double *__restrict__ gspheres, BinGrid G,
                                 DepParticles P, ShapeParams S, long long npos,
-                                double *__restrict__ out) {
+                                double *__restrict__ out,
+                                const uint32_t *__restrict__ order = nullptr) {
   __shared__ float4 ring[WARPS][2][RING];
   // per lane its positions' FP64 sums (rho, j_x, j_y, j_z per position),
   // kept in shared memory: registers go to the streaming state and the
@@ -519,8 +554,9 @@ __global__ void __launch_bounds__(BLOCK, PPL == 1 ? PRT_GATHER_MIN_BLOCKS : PRT_
   __shared__ double acc64[WARPS][4 * PPL][32];
 
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const long long g = blockIdx.x * (long long)WARPS + wid;
-  if (g >= ngroups) return;  // whole warp
+  const long long gi = blockIdx.x * (long long)WARPS + wid;
+  if (gi >= ngroups) return;  // whole warp
+  const long long g = order ? (long long)order[gi] : gi;
   const uint32_t p0 = gstarts[g];
   const int npg = (int)(gstarts[g + 1] - p0);
   float4(*R)[RING] = ring[wid];
@@ -1085,31 +1121,55 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
     long long ng;
     const uint32_t *gs;
     const double *gsp;
+    // heaviest groups first (group_work_kernel + a descending radix sort)
+    auto heavy_first = [&](long long ngr, const double *sph, const uint32_t **order) -> int {
+      *order = nullptr;
+      if (!PRT_DEPOSIT_HEAVY_FIRST || ngr < 2) return PRT_OK;
+      int rc2;
+      uint32_t *buf = (uint32_t *)ws_buffer(ws, PRT_WS_GROUP_ORDER, 16 * (size_t)ngr, &rc2);
+      if (!buf) return rc2;
+      uint32_t *wk = buf, *ids = buf + ngr, *wk_out = buf + 2 * ngr, *ids_out = buf + 3 * ngr;
+      group_work_kernel<<<prt_grid_blocks(ngr, 256), 256, 0, s>>>(ngr, sph, G, P.starts,
+                                                                  S.radius, wk, ids);
+      PRT_CHECK_CUDA(cudaGetLastError());
+      size_t tb = 0;
+      PRT_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, wk, wk_out, ids,
+                                                               ids_out, (int)ngr, 0, 32, s));
+      void *tmp = ws_buffer(ws, PRT_WS_CUB, tb, &rc2);
+      if (!tmp) return rc2;
+      PRT_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tb, wk, wk_out, ids,
+                                                               ids_out, (int)ngr, 0, 32, s));
+      *order = ids_out;
+      return PRT_OK;
+    };
+    const uint32_t *order = nullptr;
     if (precision == PRT_PRECISION_MIXED) {
       constexpr int W = PRT_MIXED_PPL;
       const unsigned nb = groups_for(W, ng, gs, gsp);
+      if ((rc = heavy_first(ng, gsp, &order))) return rc;
       if (a2)
         deposit_groups_mixed_kernel<true, W><<<nb, BLOCK, 0, s>>>(PS.pos, ng, gs, gsp, G, P, S,
-                                                                  PS.count, vals);
+                                                                  PS.count, vals, order);
       else
         deposit_groups_mixed_kernel<false, W><<<nb, BLOCK, 0, s>>>(PS.pos, ng, gs, gsp, G, P, S,
-                                                                   PS.count, vals);
+                                                                   PS.count, vals, order);
     } else {
       constexpr int W = PRT_FP64_PPL;
       const unsigned nb = groups_for(W, ng, gs, gsp);
+      if ((rc = heavy_first(ng, gsp, &order))) return rc;
       if (counter) {
         if (a2)
           deposit_groups_kernel<true, true, W><<<nb, BLOCK, 0, s>>>(
-              PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, counter);
+              PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, counter, order);
         else
           deposit_groups_kernel<false, true, W><<<nb, BLOCK, 0, s>>>(
-              PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, counter);
+              PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, counter, order);
       } else if (a2) {
         deposit_groups_kernel<true, false, W><<<nb, BLOCK, 0, s>>>(
-            PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, nullptr);
+            PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, nullptr, order);
       } else {
         deposit_groups_kernel<false, false, W><<<nb, BLOCK, 0, s>>>(
-            PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, nullptr);
+            PS.pos, ng, gs, gsp, PS.run_starts, G, P, S, PS.count, vals, nullptr, order);
       }
     }
     PRT_CHECK_CUDA(cudaGetLastError());

@@ -23,6 +23,7 @@ enum {
   PRT_WS_ADJ_PARTIALS,
   PRT_WS_DIAGNOSTICS,
   PRT_WS_AVERAGE,
+  PRT_WS_GROUP_ORDER,
   PRT_WS_SLOTS
 };
 
