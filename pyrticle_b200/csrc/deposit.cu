@@ -184,8 +184,11 @@ constexpr int WARPS = BLOCK / 32;
 #ifndef PRT_GATHER_MIN_BLOCKS_WIDE
 #define PRT_GATHER_MIN_BLOCKS_WIDE 4
 #endif
+// mixed form, wide groups: 6 CTAs (80 registers, no spills) measured best
+// with the heaviest groups first: 8 CTAs cost ~20% on dense bunches
+// (config4) and 4 CTAs ~15% on config2
 #ifndef PRT_MIXED_MIN_BLOCKS_WIDE
-#define PRT_MIXED_MIN_BLOCKS_WIDE 8
+#define PRT_MIXED_MIN_BLOCKS_WIDE 6
 #endif
 // positions per lane of the FP64 and mixed deposition (2: wide groups)
 #ifndef PRT_FP64_PPL
