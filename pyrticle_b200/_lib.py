@@ -7,7 +7,6 @@ missing or fails to load, importing anything that needs it raises.
 from __future__ import annotations
 
 import ctypes as C
-import os
 from pathlib import Path
 
 import numpy as np

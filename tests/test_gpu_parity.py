@@ -6,7 +6,6 @@ and j within 1e-12 relative L2 (FP64 plain form); deposition deterministic
 (bitwise equal on repeat).
 """
 
-import ctypes as C
 
 import numpy as np
 import pytest

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from pyrticle_b200 import meshgen, problems, refelement
-from pyrticle_b200.cloud import LSRK4_A, LSRK4_B, LSRK4_C
+from pyrticle_b200.cloud import LSRK4_A, LSRK4_B
 from pyrticle_b200.deposition.grid import (BrickInfo, basis_reduction_matrices,
                                            find_points_in_elements)
 from pyrticle_b200.tools import StatsGatherer
