@@ -251,9 +251,10 @@ def basis_reduction_matrices(mesh, order, starts, pts, w, max_condition=10.0):
                 thresh = eps * max(P, B) * ss[:, :1]
                 inv_s = np.where(np.abs(ss) >= thresh, 1.0 / np.where(ss == 0, 1, ss), 0.0)
                 k = ss.shape[1]
-                inv_diag = np.zeros((len(done), B, P))
-                inv_diag[:, np.arange(k), np.arange(k)] = inv_s
-                pinv = np.transpose(vt[g], (0, 2, 1)) @ inv_diag @ np.transpose(u[g], (0, 2, 1))
+                # V diag(1/s) U^T over the k = min(P, B) singular triplets
+                vk = np.transpose(vt[g][:, :k, :], (0, 2, 1))               # [d, B, k]
+                uk = u[g][:, :, :k]                                        # [d, P, k]
+                pinv = (vk * inv_s[:, None, :]) @ np.transpose(uk, (0, 2, 1))
                 ev = el_vdm[:, cols[g]].transpose(1, 0, 2)                  # [d, Np, B]
                 imat = ev @ pinv                                            # [d, Np, P]
                 for t, gi in enumerate(done):
@@ -281,10 +282,15 @@ def basis_reduction_matrices(mesh, order, starts, pts, w, max_condition=10.0):
 
 
 def _batched_svd(A):
+    """SVD of a batch [g, P, B]. With P >= B the thin U (P x B) suffices: the
+    pseudoinverse uses its first B columns only, and V is square either way;
+    with P < B the full V is needed (its last row spans the null space the
+    mode killing reads)."""
+    full = A.shape[1] < A.shape[2]
     try:
-        return np.linalg.svd(A, full_matrices=True)
+        return np.linalg.svd(A, full_matrices=full)
     except np.linalg.LinAlgError:
-        outs = [np.linalg.svd(a, full_matrices=True) for a in A]
+        outs = [np.linalg.svd(a, full_matrices=full) for a in A]
         return (np.stack([o[0] for o in outs]), np.stack([o[1] for o in outs]),
                 np.stack([o[2] for o in outs]))
 
