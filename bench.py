@@ -681,8 +681,8 @@ def main():
     # radix-sort kernels not counted): per sort iota + 5 permutation gathers
     # (x, p, q, m, ids; the residuals are dead at a step boundary);
     # per RK stage one fused kernel; per deposition bin keys, bin starts,
-    # payload, the gather and the expansion to nodes.
-    line["gpu_launches"] = int(kernel["lsrk_stage"][1] + 2 * kernel["deposit_gather"][1] +
+    # payload, the group work estimate, the gather and the expansion to nodes.
+    line["gpu_launches"] = int(kernel["lsrk_stage"][1] + 3 * kernel["deposit_gather"][1] +
                                3 * kernel["deposit_stage"][1] + 6 * kernel["sort"][1])
     if e2e:
         line["e2e"] = e2e
