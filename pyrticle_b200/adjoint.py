@@ -13,7 +13,8 @@ state (x, p, element, order) every ``checkpoint_every`` steps; the backward
 walks the segments in reverse, recomputes each from its checkpoint while
 recording every stage's input state (``prt_lsrk_stage_record``: bitwise the
 forward's arithmetic), then runs the stage adjoints in reverse
-(``prt_lsrk_stage_adjoint``). The deposition adjoint
+(``prt_lsrk_stage_adjoint``). The last segment is recorded by the forward
+itself, so the backward starts with its stage adjoints. The deposition adjoint
 (``prt_deposit_shape_adjoint``) and the velocity adjoint start the chain.
 Every derivative is computed by libprt's CUDA kernels; torch tensors are the
 device buffers and the autograd boundary.
@@ -151,12 +152,40 @@ class DifferentiableTrajectory:
         kx = torch.zeros_like(x)
         kp = torch.zeros_like(p)
         checkpoints = []
+        # the last segment runs recorded (prt_lsrk_stage_record, bitwise the
+        # in-place stage): its tape spares the backward that recomputation
+        last = ((self.steps - 1) // self.K) * self.K if self.steps else 0
+        Tmax = 5 * min(self.K, self.steps) if self.steps else 0
+        tape = None
+        t = 0
+        cs = C.c_void_p(stream_handle())
         for step in range(self.steps):
             if step % self.K == 0:
                 self._sort(el, x, p, q, m, kx, kp, order)
                 checkpoints.append((x.clone(), p.clone(), el.clone(), order.clone()))
+                if step == last:
+                    tape = (torch.empty((Tmax + 1, 3, n), dtype=F64, device=dev),
+                            torch.empty((Tmax + 1, 3, n), dtype=F64, device=dev),
+                            torch.empty((Tmax + 1, n), dtype=torch.int32, device=dev))
+                    tape[0][0].copy_(x)
+                    tape[1][0].copy_(p)
+                    tape[2][0].copy_(el)
+            if tape is None:
+                for a, b in zip(LSRK4_A, LSRK4_B):
+                    self._stage(Fp, x, p, q, m, el, kx, kp, a, b)
+                continue
+            tx, tp, te = tape
             for a, b in zip(LSRK4_A, LSRK4_B):
-                self._stage(Fp, x, p, q, m, el, kx, kp, a, b)
+                _lib.check(self.lib.prt_lsrk_stage_record(
+                    meth.pusher.handle, meth.workspace, n, tx[t].data_ptr(), tp[t].data_ptr(),
+                    te[t].data_ptr(), tx[t + 1].data_ptr(), tp[t + 1].data_ptr(),
+                    te[t + 1].data_ptr(), q.data_ptr(), m.data_ptr(), kx.data_ptr(),
+                    kp.data_ptr(), Fp, a, b, self.dt, self.c, cs), "prt_lsrk_stage_record")
+                t += 1
+        if tape is not None:
+            x = tape[0][t].clone()
+            p = tape[1][t].clone()
+            el = tape[2][t].clone()
         if not checkpoints:  # zero steps: the initial state is the final one
             self._sort(el, x, p, q, m, kx, kp, order)
             checkpoints.append((x.clone(), p.clone(), el.clone(), order.clone()))
@@ -170,7 +199,7 @@ class DifferentiableTrajectory:
             n, x.data_ptr(), q.data_ptr(), v.data_ptr(), el.data_ptr(), rho.data_ptr(),
             j.data_ptr(), self.precision, None, C.c_void_p(stream_handle())),
             "prt_deposit_shape")
-        saved = dict(final=(x, p, el, q, m, order, v), checkpoints=checkpoints)
+        saved = dict(final=(x, p, el, q, m, order, v), checkpoints=checkpoints, tape=tape)
         return rho, j, saved
 
     def _mark(self, marks, name):
@@ -225,9 +254,13 @@ class DifferentiableTrajectory:
         cps = saved["checkpoints"]
         cur_order = order
         Tmax = 5 * min(self.K, self.steps) if self.steps else 0
-        tx = torch.empty((Tmax + 1, 3, n), dtype=F64, device=dev)
-        tp = torch.empty((Tmax + 1, 3, n), dtype=F64, device=dev)
-        te = torch.empty((Tmax + 1, n), dtype=torch.int32, device=dev)
+        fwd_tape = saved.get("tape")
+        if fwd_tape is not None:
+            tx, tp, te = fwd_tape  # holds the last segment's stages already
+        else:
+            tx = torch.empty((Tmax + 1, 3, n), dtype=F64, device=dev)
+            tp = torch.empty((Tmax + 1, 3, n), dtype=F64, device=dev)
+            te = torch.empty((Tmax + 1, n), dtype=torch.int32, device=dev)
         kx = torch.empty_like(x)
         kp = torch.empty_like(p)
         qs = torch.empty_like(self.q)
@@ -278,6 +311,15 @@ class DifferentiableTrajectory:
                 continue
             torch.index_select(self.q, 0, order_s, out=qs)
             torch.index_select(self.m, 0, order_s, out=ms)
+            if fwd_tape is not None and seg == len(cps) - 1:
+                # recorded by the forward: the stage adjoints only
+                self._mark(marks, "carry")
+                cs = C.c_void_p(stream_handle())
+                for t in reversed(range(T)):
+                    _lib.check(lib.prt_lsrk_stage_adjoint(*adj_args[t], cs),
+                               "prt_lsrk_stage_adjoint")
+                self._mark(marks, "stage_adjoint")
+                continue
             tx[0].copy_(xs)
             tp[0].copy_(ps)
             te[0].copy_(els)

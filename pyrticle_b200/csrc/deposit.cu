@@ -202,7 +202,7 @@ constexpr int WARPS = BLOCK / 32;
 #define PRT_FP64_UNROLL 4
 #endif
 #ifndef PRT_MIXED_UNROLL
-#define PRT_MIXED_UNROLL 2
+#define PRT_MIXED_UNROLL 4
 #endif
 constexpr int FP64_UNROLL = PRT_FP64_UNROLL;
 // launch the position groups heaviest first (1) or in Morton order (0)
