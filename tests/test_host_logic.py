@@ -221,3 +221,38 @@ def test_find_counter_log_quantity():
     m.find_same_counter = 12
     assert q() == 7
     assert q() == 0
+
+
+def test_continuity_groups():
+    """average_groups (grid.py:143-183): on a non-periodic mesh every group
+    is a set of coincident nodes, and every node shared by two elements is in
+    one; on a z-periodic mesh the groups also join the nodes of the two
+    periodic faces."""
+    from pyrticle_b200 import meshgen
+    from pyrticle_b200.deposition.grid import average_groups
+    for periodic in ((False, False, False), (False, False, True)):
+        mesh = meshgen.box_mesh((3, 3, 4), (0, 0, 0), (0.01, 0.01, 0.02), periodic=periodic)
+        nodes = meshgen.element_nodes(mesh, 2)
+        starts, members = average_groups(mesh, nodes, 10)
+        assert np.all(np.diff(starts.astype(np.int64)) >= 2)
+        assert len(np.unique(members)) == len(members)
+        key = np.round(nodes / 1e-9).astype(np.int64)
+        _, inv, counts = np.unique(key, axis=0, return_inverse=True, return_counts=True)
+        shared = counts[inv.ravel()] >= 2
+        grouped = np.zeros(len(nodes), dtype=bool)
+        grouped[members] = True
+        assert np.array_equal(grouped[shared], np.ones(shared.sum(), dtype=bool))
+        z = nodes[:, 2]
+        for g in range(len(starts) - 1):
+            mem = members[starts[g]:starts[g + 1]]
+            assert np.all(np.diff(mem.astype(np.int64)) > 0)      # ascending
+            p = nodes[mem]
+            if periodic[2]:
+                p = p.copy()
+                p[:, 2] = np.where(np.isclose(p[:, 2], 0.02), 0.0, p[:, 2])
+            assert np.ptp(p, axis=0).max() < 1e-12
+        if periodic[2]:
+            joined = sum(1 for g in range(len(starts) - 1)
+                         if np.isclose(z[members[starts[g]:starts[g + 1]]], 0.0).any()
+                         and np.isclose(z[members[starts[g]:starts[g + 1]]], 0.02).any())
+            assert joined > 0  # groups span the periodic seam
