@@ -133,7 +133,8 @@ enum prt_timing_category {
   PRT_TIME_SORT = 3,           /* prt_sort_by_element */
   PRT_TIME_STAGE_ADJOINT = 4,  /* prt_lsrk_stage_adjoint kernel */
   PRT_TIME_DEPOSIT_ADJOINT = 5,/* prt_deposit_shape_adjoint */
-  PRT_TIME_CATEGORIES = 6
+  PRT_TIME_DEPOSIT_NORMALIZE = 6,/* normalising integrals of the tensor-core deposition */
+  PRT_TIME_CATEGORIES = 7
 };
 int prt_workspace_timing(prt_workspace *ws, int32_t enable);
 int prt_workspace_timing_read(prt_workspace *ws, int32_t category,
@@ -217,9 +218,19 @@ typedef struct prt_shape_function {
 /* Arithmetic of a call (`precision` arguments). */
 enum prt_precision {
   PRT_PRECISION_FP64 = 0,  /* plain form: FP64 throughout */
-  /* chosen form: deposition weights and per-batch sums in FP32, combined
-   * into FP64 per node; positions, momenta and locate stay FP64 */
-  PRT_PRECISION_MIXED = 1
+  /* chosen form. Stage: Lagrange values on the tensor cores (split BF16,
+   * FP32 accumulation), force, update and locate in FP64. Deposition (shape
+   * exponent 2): the weight max(1 - r^2/a^2, 0)^2 from a split-FP16
+   * tensor-core product with FP32 accumulation, rounded to a 16-bit integer,
+   * and summed exactly on the integer tensor cores against 48-bit integer
+   * charges (and 24-bit currents), combined into FP64 per node; the
+   * normalising integral per particle is summed exactly from the same
+   * integer weights, so deposited charge matches the particles' charge to
+   * FP64 rounding. Other exponents: as PRT_PRECISION_MIXED_SIMT. */
+  PRT_PRECISION_MIXED = 1,
+  /* deposition weights and per-batch sums in FP32 on the CUDA cores,
+   * combined into FP64 per node (deposition only) */
+  PRT_PRECISION_MIXED_SIMT = 2
 };
 
 enum prt_deposit_mode {

@@ -15,7 +15,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libprt.so"
-SOURCES = ["core.cu", "deposit.cu", "grid.cu", "adjoint.cu", "stage_mixed.cu", "diagnostics.cu", "average.cu"]
+SOURCES = ["core.cu", "deposit.cu", "deposit_tc.cu", "grid.cu", "adjoint.cu", "stage_mixed.cu", "diagnostics.cu", "average.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

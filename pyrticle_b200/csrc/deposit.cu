@@ -30,6 +30,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -841,6 +842,8 @@ int upload_vec(const std::vector<T> &v, const T **dst) {
 // ------------------------------------------------------------ position set
 
 int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
+  static std::atomic<unsigned long long> next_uid{1};
+  m->uid = next_uid++;
   const long long E = d->element_count;
   const int Np = d->nodes_per_element;
   const long long nn = E * (long long)Np;
@@ -965,6 +968,41 @@ int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
     if ((rc = upload_vec(gstart, &P.group_starts))) return rc;
     if ((rc = upload_vec(spheres, &P.group_spheres))) return rc;
 
+    // tensor-core tiles: runs of <= 128 positions cut at Morton cells of
+    // about PRT_TILE_TARGET positions, with bounding boxes
+    {
+      const double tside = std::cbrt(PRT_TILE_TARGET * vol / std::max<long long>(1, npos));
+      int tlevel = (int)std::lround(std::log2(ext / tside));
+      tlevel = std::min(std::max(tlevel, 0), 21);
+      const int tshift = 3 * (21 - tlevel);
+      std::vector<uint32_t> ts;
+      ts.reserve(npos / 64 + 2);
+      uint64_t prev_cell = ~0ull;
+      for (long long u = 0; u < npos; ++u) {
+        const uint64_t cell = key[order[run_starts[u]]] >> tshift;
+        if (u == 0 || cell != prev_cell || u - ts.back() >= 128) ts.push_back((uint32_t)u);
+        prev_cell = cell;
+      }
+      ts.push_back((uint32_t)npos);
+      const long long nt = (long long)ts.size() - 1;
+      std::vector<double> tb(6 * (size_t)std::max<long long>(1, nt), 0.0);
+      for (long long t = 0; t < nt; ++t) {
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (uint32_t p = ts[t]; p < ts[t + 1]; ++p)
+          for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], pos[3 * p + a]);
+            hi[a] = std::max(hi[a], pos[3 * p + a]);
+          }
+        for (int a = 0; a < 3; ++a) {
+          tb[6 * t + a] = 0.5 * (lo[a] + hi[a]);
+          tb[6 * t + 3 + a] = 0.5 * (hi[a] - lo[a]);
+        }
+      }
+      P.tiles = nt;
+      if ((rc = upload_vec(ts, &P.tile_starts))) return rc;
+      if ((rc = upload_vec(tb, &P.tile_boxes))) return rc;
+    }
+
     // centre bins: width about the mean group radius
     auto &CB = P.centre_bins;
     double rsum = 0, rmax = 0;
@@ -1013,6 +1051,60 @@ int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
   return PRT_OK;
 }
 
+// ------------------------------------------- pieces shared with deposit_tc.cu
+
+int prt_dep_position_weights(const prt_mesh *mesh, prt_workspace *ws, const double *iw,
+                             double *W, cudaStream_t s) {
+  int rc;
+  double *iwd = (double *)ws_buffer(ws, PRT_WS_DEP_STATS,
+                                    sizeof(double) * (64 + mesh->dev.Np + 10 * STATS_BLOCKS), &rc);
+  if (!iwd) return rc;
+  PRT_CHECK_CUDA(cudaMemcpyAsync(iwd, iw, sizeof(double) * mesh->dev.Np, cudaMemcpyHostToDevice, s));
+  const PositionSet &PS = mesh->positions;
+  position_weights_kernel<<<prt_grid_blocks(PS.count, 256), 256, 0, s>>>(
+      PS.count, PS.run_starts, PS.run_nodes, mesh->dev.Np, iwd, mesh->dev.jacobians, W);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  return PRT_OK;
+}
+
+int prt_dep_norm_stats(prt_workspace *ws, long long n, const double *scale, const double *hits,
+                       prt_deposit_stats *stats, cudaStream_t s) {
+  int rc;
+  double *aux = (double *)ws_buffer(ws, PRT_WS_DEP_COUNT, sizeof(double) * (16 + 10 * STATS_BLOCKS), &rc);
+  if (!aux) return rc;
+  const long long need = (n + 255) / 256;
+  const int sb = (int)(need < 1 ? 1 : need < STATS_BLOCKS ? need : STATS_BLOCKS);
+  double *partials = aux + 16;
+  stats_kernel<<<sb, 256, 0, s>>>(n, scale, hits, partials);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  stats_final_kernel<<<1, 32, 0, s>>>(sb, partials, aux);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  double h[10];
+  PRT_CHECK_CUDA(cudaMemcpyAsync(h, aux, sizeof(h), cudaMemcpyDeviceToHost, s));
+  PRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  stats->norm_count = h[0];
+  stats->norm_sum = h[1];
+  stats->norm_sum_sq = h[2];
+  stats->norm_min = h[3];
+  stats->norm_max = h[4];
+  stats->el_count = h[5];
+  stats->el_sum = h[6];
+  stats->el_sum_sq = h[7];
+  stats->el_min = h[8];
+  stats->el_max = h[9];
+  return PRT_OK;
+}
+
+int prt_dep_expand(const prt_mesh *mesh, const double *vals, double *rho, double *j,
+                   cudaStream_t s) {
+  if (!rho && !j) return PRT_OK;
+  const long long nn = mesh->dev.E * (long long)mesh->dev.Np;
+  expand_kernel<<<prt_grid_blocks(nn, 256), 256, 0, s>>>(nn, mesh->positions.count,
+                                                         mesh->positions.node_to_pos, vals, rho, j);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  return PRT_OK;
+}
+
 // -------------------------------------------------------------- C ABI: mesh
 
 extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
@@ -1022,13 +1114,18 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
                                  int32_t precision, prt_deposit_stats *stats,
                                  void *stream) {
   if (!mesh || !ws || n < 0 || n >= (1ll << 31)) return PRT_ERR_INVALID_ARGUMENT;
-  if (precision != PRT_PRECISION_FP64 && precision != PRT_PRECISION_MIXED)
+  if (precision != PRT_PRECISION_FP64 && precision != PRT_PRECISION_MIXED &&
+      precision != PRT_PRECISION_MIXED_SIMT)
     return PRT_ERR_INVALID_ARGUMENT;
   if (!(shape.radius > 0) || (mode != PRT_DEPOSIT_PLAIN && mode != PRT_DEPOSIT_NORMALIZED))
     return PRT_ERR_INVALID_ARGUMENT;
   if (mode == PRT_DEPOSIT_NORMALIZED && !iw) return PRT_ERR_INVALID_ARGUMENT;
   if (n > 0 && (!x || !q || (j && !v))) return PRT_ERR_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;
+  // the chosen form runs on the tensor cores for the alpha = 2 shape; other
+  // exponents take the CUDA-core form
+  if (precision == PRT_PRECISION_MIXED && shape.alpha == 2 && n > 0)
+    return prt_deposit_shape_tc(mesh, ws, mode, shape, iw, n, x, q, v, el, rho, j, stats, s);
   const long long nn = mesh->dev.E * (long long)mesh->dev.Np;
   const PositionSet &PS = mesh->positions;
   if (stats) std::memset(stats, 0, sizeof(*stats));
@@ -1146,7 +1243,7 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
       return PRT_OK;
     };
     const uint32_t *order = nullptr;
-    if (precision == PRT_PRECISION_MIXED) {
+    if (precision != PRT_PRECISION_FP64) {
       constexpr int W = PRT_MIXED_PPL;
       const unsigned nb = groups_for(W, ng, gs, gsp);
       if ((rc = heavy_first(ng, gsp, &order))) return rc;

@@ -1,0 +1,1080 @@
+// deposit_tc.cu -- the chosen-form shape deposition on the tensor cores.
+//
+// The reference deposits q S(x_node - x_p) particle by particle over the
+// elements its walk reaches (dep_shape.hpp:128-149), and the normalising
+// depositor first integrates each particle's shape over the nodes it reaches,
+// sum_e |J_e| sum_i w_i S_i, and deposits q / integral instead of q
+// (dep_normshape.hpp:125-199). Both are sums over (particle, node position)
+// pairs within the radius a of S(r) = N (a - r^2/a)^2 = N a^2 (1 - r^2/a^2)^2.
+//
+// Here the distinct node positions are cut into tiles of <= 128 (Morton
+// runs, PositionSet::tiles) and each CTA takes one tile:
+//
+//  1. candidates: the particles of the bin rows within the radius of the
+//     tile's box (particles binned and packed in bin order, binning.cuh),
+//     culled against the box grown by the radius, are staged 128 at a time
+//     (a chunk) in a shared-memory ring by all eight warps;
+//  2. score: one tcgen05.mma (kind::f16, M = 128 positions, N = 128
+//     candidates, K = 16) gives s = SIGMA (1 - |u - w|^2 / a^2) for every
+//     pair, with u and w the coordinates relative to the tile centre. The
+//     operands are split into two FP16 terms (x = x_h + x_l) and laid out so
+//     that one K = 16 product sums u_h v_h + u_h v_l + u_l v_h for the three
+//     coordinates (v = 2 SIGMA w), the position term SIGMA (1 - |u|^2) and
+//     the particle term -SIGMA |w|^2, each as two terms; the tensor cores
+//     accumulate in FP32 into tensor memory;
+//  3. weight: each thread reads its position's row (tcgen05.ld), forms
+//     t = s + |s| = 2 max(s, 0) and the integer F = round(t^2) =
+//     round(4 SIGMA^2 max(1 - r^2/a^2, 0)^2) <= 65525 with one FMA
+//     (t t + 2^23 puts the rounded integer in the low mantissa bits), and
+//     stores its two bytes as unsigned 8-bit digits in shared memory;
+//  4. sums: tcgen05.mma kind::i8 (int32 accumulation in tensor memory,
+//     exact) of the weight digits against
+//      - deposition: per candidate the charge c (q or q / integral) as a
+//        48-bit integer in six balanced signed digits and c v (each
+//        component 24 bits, three digits), one 16-column operand; rows =
+//        positions, so tensor memory accumulates sum_p F c per position over
+//        the whole tile (folded into FP64 every 256 chunks before int32
+//        could overflow);
+//      - normalisation: per position the weight sum_{nodes} |J_e| w_i as a
+//        48-bit integer in six unsigned digits; the weight digits are read
+//        transposed (MN-major: the same bytes are rows = candidates), so the
+//        product is, per candidate, sum_u F W over the tile, which the CTA
+//        adds to the particle's integral as two exact 64-bit integer atomics
+//        (high and low part): integer sums do not depend on the order, so the
+//        result is deterministic.
+//     The weights F of both passes are bitwise the same (same tiles, same
+//     operands, same instructions), and every sum of F is exact, so the
+//     deposited charge sum_u W_u rho_u equals sum_p q_p up to the 48-bit
+//     representation of W and c and the final FP64 roundings (~1e-16).
+//
+// Synchronisation per chunk k of a CTA: the score MMA of chunk k runs while
+// the warps stage chunk k+1; the weights of chunk k are written once the
+// accumulation MMA of chunk k-1 has completed (mbarrier); one thread issues
+// the accumulation MMA of chunk k and the score MMA of chunk k+1. Every
+// mbarrier wait is bounded: a CTA whose wait runs out records PRT_ERR_TIMEOUT,
+// stops, waits (bounded) for its issued MMAs and frees its tensor memory.
+
+#include <cuda_fp16.h>
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <cstring>
+
+#include "binning.cuh"
+
+namespace {
+
+using namespace prt_dep;
+
+constexpr int TM = 128;          // positions per tile: MMA M, tensor-memory lanes
+constexpr int NC = 128;          // candidates per chunk: score MMA N
+constexpr int RING = 512;        // candidate slots in shared memory
+constexpr int THREADS = 256;     // eight warps
+constexpr int MAXSEG = 512;      // bin-row segments per tile
+constexpr uint32_t TMEM_COLS = 256;
+constexpr uint32_t COL_ACC = 128;  // accumulators: high digit +0, low digit +16, indicator +32
+constexpr float SIGMA = 127.99f;   // 4 SIGMA^2 < 65536
+constexpr unsigned SPIN = 1u << 22;  // try_wait rounds before a wait gives up
+constexpr int FLUSH_CHUNKS = 256;    // int32 accumulation window (256 * 128 * 255 * 128 < 2^31)
+constexpr int CDIG = 6, JDIG = 3, WDIG = 6;
+
+struct Smem {
+  uint8_t apos[2 * TM * 16];     // position operand, K-major: [K chunk][row][16 B]
+  uint8_t bcand[2 * RING * 16];  // candidate operands, K-major: [K chunk][slot][16 B]
+  uint8_t bdig[RING * 16];       // charge digits per slot (16 columns, MN-major)
+  uint8_t wdig[TM * 16];         // weight digits per position (16 columns, MN-major)
+  // weight digits: [high, low, indicator][16-candidate block][position][16 B]
+  uint8_t fdig[3][NC / 16][TM][16];
+  uint32_t slot_id[RING];        // bin-order particle of a slot (normalisation)
+  uint32_t seg_start[MAXSEG];    // first bin-order particle of a segment
+  uint32_t seg_pref[MAXSEG + 1]; // stream offset of a segment
+  uint8_t seg_img[MAXSEG];       // periodic image (qx+1) + 3 (qy+1) + 9 (qz+1)
+  unsigned long long bar_s, bar_a;
+  uint32_t tmem;
+  int tail, cursor, nseg, total, abort;
+};
+// 2 CTAs per SM at most (2 x 256 tensor-memory columns = all 512)
+static_assert(sizeof(Smem) + 1024 > 228 * 1024 / 3, "shared memory keeps tensor memory within one SM");
+
+struct TcArgs {
+  BinGrid G;
+  const double2 *__restrict__ pay;      // [n][4] bin-order payload (x, y | z, q | ...)
+  const uint32_t *__restrict__ starts;  // [nbins + 1]
+  const uint32_t *__restrict__ tile_starts;
+  const double *__restrict__ tile_boxes;
+  const uint4 *__restrict__ tile_ops;   // [tiles][256] position operands
+  const uint4 *__restrict__ wdig;       // [tiles][128] weight digits
+  const uint4 *__restrict__ cdig;       // [n] charge digits, bin order
+  const uint32_t *__restrict__ order;   // launch order of the tiles (or NULL)
+  double radius, inv_radius;
+  unsigned long long *__restrict__ norm_hi, *__restrict__ norm_lo;  // [n], bin order
+  uint32_t *__restrict__ hits;                                      // [n], bin order
+  const double *__restrict__ out_scale;  // [4]: rho, jx, jy, jz factors
+  double *__restrict__ vals;             // [4][npos]
+  long long npos;
+  unsigned long long *__restrict__ counters;  // [0]: candidates over all tiles
+  DevStatus *st;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// tcgen05 shared-memory matrix descriptor, no swizzle
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version of this architecture
+  return d;
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                        uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (unsigned k = 0; k < SPIN; ++k) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(addr)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// FP32 -> (high, low) FP16 terms
+__device__ __forceinline__ void split_half(float x, __half &h, __half &l) {
+  h = __float2half_rn(x);
+  l = __float2half_rn(x - __half2float(h));
+}
+
+__device__ __forceinline__ uint32_t pack2(__half a, __half b) {
+  return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
+}
+
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+  return d;
+}
+
+// The candidate operand of a particle at w (relative to the tile centre, in
+// units of the radius), K = 16 halves:
+//   [vx_h, vx_l, vx_h, vy_h, vy_l, vy_h, vz_h, vz_l, vz_h, 1, 1, g_h, g_l, 0, 0, 0]
+// with v = 2 SIGMA w and g = -SIGMA |w|^2; the position operand is
+//   [ux_h, ux_h, ux_l, uy_h, uy_h, uy_l, uz_h, uz_h, uz_l, b_h, b_l, 1, 1, 0, 0, 0]
+// with b = SIGMA (1 - |u|^2), so the product is
+//   u.v + b + g = SIGMA (1 - |u - w|^2) (up to the dropped low x low terms).
+__device__ __forceinline__ void candidate_operand(float w0, float w1, float w2, uint4 &k0,
+                                                  uint4 &k1) {
+  __half h[3], l[3], gh, gl;
+  split_half(2.0f * SIGMA * w0, h[0], l[0]);
+  split_half(2.0f * SIGMA * w1, h[1], l[1]);
+  split_half(2.0f * SIGMA * w2, h[2], l[2]);
+  split_half(-SIGMA * fmaf(w0, w0, fmaf(w1, w1, w2 * w2)), gh, gl);
+  const __half one = __float2half_rn(1.0f), zero = __float2half_rn(0.0f);
+  k0 = make_uint4(pack2(h[0], l[0]), pack2(h[0], h[1]), pack2(l[1], h[1]), pack2(h[2], l[2]));
+  k1 = make_uint4(pack2(h[2], one), pack2(one, gh), pack2(gl, zero), pack2(zero, zero));
+}
+
+// Bin-row segments of a tile (warp 0): every run of bins along x, in the
+// rows (bz, by) within the radius of the box [c - hf, c + hf], as ranges of
+// bin-order particles with their periodic image; the stream of candidates
+// is the concatenation of the segments.
+__device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], const double hf[3],
+                               int lane) {
+  const BinGrid &G = A.G;
+  const double rr = A.radius * (1 + 1e-5), rr2 = rr * rr;
+  int ulo[3], uhi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    ulo[d] = bin_floor(G, d, c[d] - hf[d] - A.radius);
+    uhi[d] = bin_floor(G, d, c[d] + hf[d] + A.radius);
+    if (G.periodic[d]) {
+      ulo[d] -= 1;
+      uhi[d] += 1;
+    } else {
+      ulo[d] = max(ulo[d], 0);
+      uhi[d] = min(uhi[d], G.dims[d] - 1);
+    }
+  }
+  auto slab_gap = [&](int d, double blo) {
+    const double e =
+        fmax(0.0, fmax(blo - (c[d] + hf[d]), (c[d] - hf[d]) - (blo + G.w[d]))) - G.slack[d];
+    return e > 0 ? e * e : 0.0;
+  };
+  const int ny = max(0, uhi[1] - ulo[1] + 1), nz = max(0, uhi[2] - ulo[2] + 1);
+  const int nrows = ny * nz;
+  int nseg = 0;
+  uint32_t total = 0;
+  bool overflow = false;
+  for (int r0 = 0; r0 < nrows; r0 += 32) {
+    const int r = r0 + lane;
+    uint32_t s_start[3], s_len[3];
+    uint8_t s_img[3];
+    int cnt = 0;
+    uint32_t len = 0;
+    if (r < nrows) {
+      const int bz = ulo[2] + r / ny, by = ulo[1] + r % ny;
+      int wz = bz, qz = 0, wy = by, qy = 0;
+      if (G.periodic[2]) {
+        qz = floor_div(bz, G.dims[2]);
+        wz = bz - qz * G.dims[2];
+      }
+      if (G.periodic[1]) {
+        qy = floor_div(by, G.dims[1]);
+        wy = by - qy * G.dims[1];
+      }
+      const double dyz2 = slab_gap(2, G.origin[2] + bz * G.w[2]) +
+                          slab_gap(1, G.origin[1] + by * G.w[1]);
+      if (dyz2 <= rr2) {
+        const double rem = sqrt(rr2 - dyz2);
+        int bx0 = bin_floor(G, 0, c[0] - hf[0] - rem);
+        int bx1 = bin_floor(G, 0, c[0] + hf[0] + rem);
+        if (G.periodic[0]) {
+          bx0 -= 1;
+          bx1 += 1;
+        }
+        bx0 = max(bx0, ulo[0]);
+        bx1 = min(bx1, uhi[0]);
+        const long long row = (long long)G.dims[0] * (wy + (long long)G.dims[1] * wz);
+        int bx = bx0;
+        while (bx <= bx1) {
+          int wx = bx, qx = 0, seg_end = bx1;
+          if (G.periodic[0]) {
+            qx = floor_div(bx, G.dims[0]);
+            wx = bx - qx * G.dims[0];
+            seg_end = min(bx1, (qx + 1) * G.dims[0] - 1);
+          }
+          const uint32_t s0 = A.starts[row + wx];
+          const uint32_t s1 = A.starts[row + wx + (seg_end - bx) + 1];
+          bx = seg_end + 1;
+          if (s1 > s0) {
+            if (cnt < 3) {
+              s_start[cnt] = s0;
+              s_len[cnt] = s1 - s0;
+              s_img[cnt] = (uint8_t)((qx + 1) + 3 * (qy + 1) + 9 * (qz + 1));
+              len += s1 - s0;
+              ++cnt;
+            } else {
+              overflow = true;
+            }
+          }
+        }
+      }
+    }
+    // exclusive warp scans of the segment counts and lengths
+    int cs = cnt;
+    uint32_t ls = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int c2 = __shfl_up_sync(0xffffffffu, cs, o);
+      const uint32_t l2 = __shfl_up_sync(0xffffffffu, ls, o);
+      if (lane >= o) {
+        cs += c2;
+        ls += l2;
+      }
+    }
+    const int sbase = nseg + cs - cnt;
+    uint32_t lbase = total + ls - len;
+    for (int i = 0; i < cnt; ++i) {
+      if (sbase + i < MAXSEG) {
+        S.seg_start[sbase + i] = s_start[i];
+        S.seg_pref[sbase + i] = lbase;
+        S.seg_img[sbase + i] = s_img[i];
+      }
+      lbase += s_len[i];
+    }
+    nseg += __shfl_sync(0xffffffffu, cs, 31);
+    total += __shfl_sync(0xffffffffu, ls, 31);
+  }
+  overflow = __any_sync(0xffffffffu, overflow) || nseg > MAXSEG;
+  if (lane == 0) {
+    S.nseg = overflow ? 0 : nseg;
+    S.total = overflow ? 0 : (int)total;
+    S.seg_pref[overflow ? 0 : nseg] = overflow ? 0 : total;
+    if (overflow) {
+      S.abort = 1;
+      record_error(A.st, PRT_ERR_CAPACITY, -1);
+    }
+  }
+}
+
+// Stages candidates into the ring until it holds `target` slots or the
+// stream ends (every warp; at most 32 slots per warp past the target).
+template <bool NORM>
+__device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const double c[3],
+                                     const float hf[3], int target, int lane) {
+  const BinGrid &G = A.G;
+  const float rcf = (float)(A.radius * (1 + 1e-5));
+  const float rc4 = 4.0f * rcf * rcf;
+  const float inv_a = (float)A.inv_radius;
+  const int total = S.total, nseg = S.nseg;
+  for (;;) {
+    const int tail = __shfl_sync(0xffffffffu, *(volatile int *)&S.tail, 0);
+    if (tail >= target) break;
+    int t0 = 0;
+    if (lane == 0) t0 = atomicAdd(&S.cursor, 32);
+    t0 = __shfl_sync(0xffffffffu, t0, 0);
+    if (t0 >= total) break;
+    const int idx = t0 + lane;
+    bool in = false;
+    float w0 = 0, w1 = 0, w2 = 0;
+    uint32_t k = 0;
+    if (idx < total) {
+      int lo = 0, hi = nseg - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((int)S.seg_pref[mid] <= idx)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      k = S.seg_start[lo] + (uint32_t)(idx - (int)S.seg_pref[lo]);
+      const int img = S.seg_img[lo];
+      const double sx = (img % 3 - 1) * G.period[0] - c[0];
+      const double sy = ((img / 3) % 3 - 1) * G.period[1] - c[1];
+      const double sz = (img / 9 - 1) * G.period[2] - c[2];
+      const double2 xy = A.pay[4 * (size_t)k], zq = A.pay[4 * (size_t)k + 1];
+      w0 = (float)(xy.x + sx);
+      w1 = (float)(xy.y + sy);
+      w2 = (float)(zq.x + sz);
+      // rounded-box cull: per axis 2 max(|w| - half, 0) = d + |d|
+      const float d0 = fabsf(w0) - hf[0], d1 = fabsf(w1) - hf[1], d2 = fabsf(w2) - hf[2];
+      const float e0 = d0 + fabsf(d0), e1 = d1 + fabsf(d1), e2 = d2 + fabsf(d2);
+      in = e0 * e0 + e1 * e1 + e2 * e2 <= rc4;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, in);
+    int base = 0;
+    if (lane == 0 && bal) base = atomicAdd(&S.tail, __popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (in) {
+      const int slot = (base + __popc(bal & ((1u << lane) - 1u))) & (RING - 1);
+      uint4 k0, k1;
+      candidate_operand(w0 * inv_a, w1 * inv_a, w2 * inv_a, k0, k1);
+      *reinterpret_cast<uint4 *>(S.bcand + (size_t)slot * 16) = k0;
+      *reinterpret_cast<uint4 *>(S.bcand + (size_t)(RING + slot) * 16) = k1;
+      if (NORM)
+        S.slot_id[slot] = k;
+      else
+        *reinterpret_cast<uint4 *>(S.bdig + (size_t)slot * 16) = A.cdig[k];
+    }
+  }
+}
+
+// Zeroes the candidate operands of slots [from, to) of a ring chunk (the
+// tail of the last chunk): a zero operand gives score 0, weight 0.
+__device__ __forceinline__ void pad_chunk(Smem &S, int from, int to, int tid) {
+  for (int i = from + tid; i < to; i += THREADS) {
+    const int slot = i & (RING - 1);
+    *reinterpret_cast<uint4 *>(S.bcand + (size_t)slot * 16) = make_uint4(0, 0, 0, 0);
+    *reinterpret_cast<uint4 *>(S.bcand + (size_t)(RING + slot) * 16) = make_uint4(0, 0, 0, 0);
+    *reinterpret_cast<uint4 *>(S.bdig + (size_t)slot * 16) = make_uint4(0, 0, 0, 0);
+  }
+}
+
+// Weight digits of one chunk from its scores in tensor memory: thread
+// (warp w, lane l) takes position row 32 (w % 4) + l and candidate columns
+// 64 (w / 4) .. + 63.
+template <bool IND>
+__device__ __forceinline__ void weights(Smem &S, uint32_t tmem, int warp, int lane) {
+  const int q = warp & 3, h = warp >> 2;
+  const int row = 32 * q + lane;
+#pragma unroll 1
+  for (int half = 0; half < 2; ++half) {
+    uint32_t r[32];
+    tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(64 * h + 32 * half), r);
+    tmem_wait_ld();
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      uint32_t lo[4], hi[4], ind[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        uint32_t b[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float s = __uint_as_float(r[16 * g + 4 * j + e]);
+          const float t = s + fabsf(s);                     // 2 max(s, 0), exact
+          b[e] = __float_as_uint(fmaf(t, t, 8388608.0f));  // 2^23 + round(t^2)
+        }
+        const uint32_t x = prmt(b[0], b[1], 0x5140), y = prmt(b[2], b[3], 0x5140);
+        lo[j] = prmt(x, y, 0x5410);  // byte 0 of each value
+        hi[j] = prmt(x, y, 0x7632);  // byte 1 of each value
+        if (IND) ind[j] = __vcmpne4(lo[j] | hi[j], 0u) & 0x01010101u;
+      }
+      const int blk = (64 * h + 32 * half + 16 * g) >> 4;
+      *reinterpret_cast<uint4 *>(&S.fdig[0][blk][row][0]) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+      *reinterpret_cast<uint4 *>(&S.fdig[1][blk][row][0]) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+      if (IND)
+        *reinterpret_cast<uint4 *>(&S.fdig[2][blk][row][0]) =
+            make_uint4(ind[0], ind[1], ind[2], ind[3]);
+    }
+  }
+}
+
+// Instruction descriptors (M = 128):
+//  score: D FP32, A/B FP16, both K-major, N = 128
+constexpr uint32_t IDESC_SCORE =
+    (1u << 4) | ((uint32_t)(NC >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+//  deposition sums: D S32, A U8 K-major (weights, rows = positions), B S8
+//  MN-major (charge digits), N = 16
+constexpr uint32_t IDESC_DEP = (2u << 4) | (1u << 10) | (1u << 16) | (2u << 17) | (8u << 24);
+//  normalisation sums: D S32, A U8 MN-major (weights read as rows =
+//  candidates), B U8 MN-major (position weight digits), N = 16
+constexpr uint32_t IDESC_NORM = (2u << 4) | (1u << 15) | (1u << 16) | (2u << 17) | (8u << 24);
+
+template <bool NORM, bool IND>
+__global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long tile = A.order ? (long long)A.order[blockIdx.x] : (long long)blockIdx.x;
+  const uint32_t p0 = A.tile_starts[tile];
+  const int npt = (int)(A.tile_starts[tile + 1] - p0);
+  double c[3], hfd[3];
+  float hf[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    c[d] = A.tile_boxes[6 * tile + d];
+    hfd[d] = A.tile_boxes[6 * tile + 3 + d] + 1e-5 * A.radius;
+    hf[d] = (float)hfd[d];
+  }
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&S.tmem)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.bar_s)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.bar_a)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    S.tail = 0;
+    S.cursor = 0;
+    S.abort = 0;
+  }
+  {
+    const uint4 *src = A.tile_ops + (size_t)tile * 256;
+    for (int i = tid; i < 256; i += THREADS) reinterpret_cast<uint4 *>(S.apos)[i] = src[i];
+    if (NORM) {
+      const uint4 *ws = A.wdig + (size_t)tile * 128;
+      for (int i = tid; i < 128; i += THREADS) reinterpret_cast<uint4 *>(S.wdig)[i] = ws[i];
+    }
+  }
+  __syncthreads();
+  if (warp == 0) build_segments(S, A, c, hfd, lane);
+  fence_async_smem();
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = S.tmem;
+  const uint32_t bar_s = smem_u32(&S.bar_s), bar_a = smem_u32(&S.bar_a);
+  const uint32_t a_pos = smem_u32(S.apos), b_cand = smem_u32(S.bcand), b_dig = smem_u32(S.bdig);
+  const uint32_t w_dig = smem_u32(S.wdig), f_dig = smem_u32(S.fdig);
+
+  // per thread: position row 32 (warp % 4) + lane, digit warp / 4 of the
+  // deposition's accumulators (FP64 across int32 windows)
+  double acc[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) acc[i] = 0;
+
+  bool ok = S.abort == 0;
+  int issued_s = 0, issued_a = 0, waited_s = 0, waited_a = 0;
+  int valid = 0;
+
+  // readout of a normalisation chunk: per candidate its sum over the tile
+  auto norm_readout = [&](int chunk, int nvalid) {
+    if (warp < 4) {
+      uint32_t d1[16], d0[16], di[16];
+      const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+      tmem_ld16(lane_addr + COL_ACC, d1);
+      tmem_ld16(lane_addr + COL_ACC + 16, d0);
+      if (IND) tmem_ld16(lane_addr + COL_ACC + 32, di);
+      tmem_wait_ld();
+      const int cr = 32 * warp + lane;
+      if (cr < nvalid) {
+        unsigned __int128 P = 0;
+#pragma unroll
+        for (int kk = 0; kk < WDIG; ++kk)
+          P += ((unsigned __int128)d1[kk] << (8 * kk + 8)) + ((unsigned __int128)d0[kk] << (8 * kk));
+        const uint32_t id = S.slot_id[(chunk * NC + cr) & (RING - 1)];
+        if (P != 0) {
+          atomicAdd(A.norm_hi + id, (unsigned long long)(P >> 40));
+          atomicAdd(A.norm_lo + id, (unsigned long long)(P & ((1ull << 40) - 1)));
+        }
+        if (IND && di[WDIG]) atomicAdd(A.hits + id, di[WDIG]);
+      }
+    }
+  };
+  // deposition accumulators -> FP64
+  auto dep_fold = [&]() {
+    uint32_t d[16];
+    tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + COL_ACC + 16 * (warp >> 2), d);
+    tmem_wait_ld();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) acc[i] += (double)(int)d[i];
+  };
+  auto wait_s = [&]() {
+    const bool w = mbar_wait(bar_s, (uint32_t)(waited_s & 1));
+    ++waited_s;
+    return __syncthreads_and(w) != 0;
+  };
+  auto wait_a = [&]() {
+    const bool w = mbar_wait(bar_a, (uint32_t)(waited_a & 1));
+    ++waited_a;
+    return __syncthreads_and(w) != 0;
+  };
+
+  int window = 0;       // chunks in the current int32 deposition window
+  int valid_prev = 0;   // valid slots of the chunk whose accumulation is in flight
+  if (ok) {
+    fill<NORM>(S, A, c, hf, NC, lane);
+    __syncthreads();
+    valid = min(S.tail, NC);
+    if (valid > 0 && valid < NC) pad_chunk(S, valid, NC, tid);
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    if (valid > 0 && tid == 0) {
+      fence_after();
+      mma_f16(tmem, sdesc(a_pos, TM * 16, 128), sdesc(b_cand, RING * 16, 128), IDESC_SCORE, 0);
+      mma_commit(bar_s);
+    }
+    if (valid > 0) ++issued_s;
+  }
+  for (int k = 0; ok && valid > 0; ++k) {
+    // (1) the accumulation of chunk k-1 is complete: its operands may be
+    // overwritten; read the normalisation sums, or fold a full window
+    if (k > 0) {
+      ok = wait_a();
+      if (!ok) break;
+      fence_after();
+      if (NORM) {
+        norm_readout(k - 1, valid_prev);
+      } else if (window == FLUSH_CHUNKS) {
+        dep_fold();
+        window = 0;
+      }
+    }
+    __syncthreads();
+    // (2) stage chunk k+1 while the tensor cores score chunk k
+    fill<NORM>(S, A, c, hf, (k + 2) * NC, lane);
+    __syncthreads();
+    const int valid_next = min(max(S.tail - (k + 1) * NC, 0), NC);
+    if (valid_next > 0 && valid_next < NC)
+      pad_chunk(S, (k + 1) * NC + valid_next, (k + 2) * NC, tid);
+    // (3) the weights of chunk k
+    ok = wait_s();
+    if (!ok) break;
+    fence_after();
+    weights<NORM && IND>(S, tmem, warp, lane);
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    // (4) the sums of chunk k, the scores of chunk k+1
+    if (tid == 0) {
+      fence_after();
+      const int slot0 = (k * NC) & (RING - 1);
+      if (NORM) {
+#pragma unroll
+        for (int d = 0; d < (IND ? 3 : 2); ++d)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj)
+            mma_i8(tmem + COL_ACC + 16 * d,
+                   sdesc(f_dig + d * (NC / 16) * TM * 16 + jj * 512, 128, (uint32_t)TM * 16),
+                   sdesc(w_dig + jj * 512, 128, 128), IDESC_NORM, jj > 0);
+      } else {
+#pragma unroll
+        for (int d = 0; d < 2; ++d)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj)
+            mma_i8(tmem + COL_ACC + 16 * d,
+                   sdesc(f_dig + d * (NC / 16) * TM * 16 + jj * 2 * TM * 16, TM * 16, 128),
+                   sdesc(b_dig + (slot0 + 32 * jj) * 16, 128, 128), IDESC_DEP,
+                   (window > 0 || jj > 0) ? 1u : 0u);
+      }
+      mma_commit(bar_a);
+      if (valid_next > 0) {
+        const int slot1 = ((k + 1) * NC) & (RING - 1);
+        mma_f16(tmem, sdesc(a_pos, TM * 16, 128), sdesc(b_cand + slot1 * 16, RING * 16, 128),
+                IDESC_SCORE, 0);
+        mma_commit(bar_s);
+      }
+    }
+    ++issued_a;
+    if (valid_next > 0) ++issued_s;
+    ++window;
+    valid_prev = valid;
+    valid = valid_next;
+  }
+  // the last chunk's sums
+  if (ok && issued_a > waited_a) {
+    ok = wait_a();
+    if (ok) {
+      fence_after();
+      if (NORM)
+        norm_readout(issued_a - 1, valid_prev);
+      else
+        dep_fold();
+    }
+  }
+  if (!ok) {
+    // a wait ran out: record it, let the issued MMAs finish (bounded), stop
+    if (tid == 0 && S.abort == 0) record_error(A.st, PRT_ERR_TIMEOUT, tile);
+    while (waited_s < issued_s) {
+      mbar_wait(bar_s, (uint32_t)(waited_s & 1));
+      ++waited_s;
+    }
+    while (waited_a < issued_a) {
+      mbar_wait(bar_a, (uint32_t)(waited_a & 1));
+      ++waited_a;
+    }
+  } else {
+    if (tid == 0) atomicAdd(A.counters, (unsigned long long)S.tail);
+    if (!NORM) {
+      // per position: T_i = 256 (high-digit sum) + (low-digit sum), then the
+      // charge (six digits) and current (three digits per component)
+      double(*lo_acc)[16] = reinterpret_cast<double(*)[16]>(&S.fdig[0][0][0][0]);
+      const int row = 32 * (warp & 3) + lane;
+      if (warp >= 4) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) lo_acc[row][i] = acc[i];
+      }
+      __syncthreads();
+      if (warp < 4 && row < npt) {
+        double T[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) T[i] = fma(256.0, acc[i], lo_acc[row][i]);
+        double r = T[CDIG - 1];
+#pragma unroll
+        for (int i = CDIG - 2; i >= 0; --i) r = fma(r, 256.0, T[i]);
+        double jc[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const int b = CDIG + JDIG * d;
+          jc[d] = fma(fma(T[b + 2], 256.0, T[b + 1]), 256.0, T[b]);
+        }
+        const long long u = p0 + row;
+        A.vals[u] = r * A.out_scale[0];
+        A.vals[A.npos + u] = jc[0] * A.out_scale[1];
+        A.vals[2 * A.npos + u] = jc[1] * A.out_scale[2];
+        A.vals[3 * A.npos + u] = jc[2] * A.out_scale[3];
+      }
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS)
+                 : "memory");
+  }
+}
+
+// ------------------------------------------------------------ preparation
+
+// Position operands of every tile, K-major: row u of tile t at
+// [t][K chunk][u][16 B] (rows past the tile's positions are zero).
+__global__ void tile_operands_kernel(long long tiles, const uint32_t *__restrict__ tile_starts,
+                                     const double *__restrict__ tile_boxes,
+                                     const double *__restrict__ pos, double inv_radius,
+                                     uint4 *__restrict__ out) {
+  const long long t = blockIdx.x;
+  const int u = threadIdx.x;
+  if (t >= tiles) return;
+  const uint32_t p0 = tile_starts[t];
+  const int npt = (int)(tile_starts[t + 1] - p0);
+  uint4 k0 = make_uint4(0, 0, 0, 0), k1 = make_uint4(0, 0, 0, 0);
+  if (u < npt) {
+    const long long p = p0 + u;
+    const double ux = (pos[3 * p] - tile_boxes[6 * t]) * inv_radius;
+    const double uy = (pos[3 * p + 1] - tile_boxes[6 * t + 1]) * inv_radius;
+    const double uz = (pos[3 * p + 2] - tile_boxes[6 * t + 2]) * inv_radius;
+    const double b = (double)SIGMA * (1.0 - (ux * ux + uy * uy + uz * uz));
+    __half xh, xl, yh, yl, zh, zl, bh, bl;
+    split_half((float)ux, xh, xl);
+    split_half((float)uy, yh, yl);
+    split_half((float)uz, zh, zl);
+    split_half((float)b, bh, bl);
+    const __half one = __float2half_rn(1.0f), zero = __float2half_rn(0.0f);
+    k0 = make_uint4(pack2(xh, xh), pack2(xl, yh), pack2(yh, yl), pack2(zh, zh));
+    k1 = make_uint4(pack2(zl, bh), pack2(bl, one), pack2(one, zero), pack2(zero, zero));
+  }
+  out[256 * t + u] = k0;
+  out[256 * t + 128 + u] = k1;
+}
+
+__device__ __forceinline__ void atomic_max_abs(unsigned long long *m, double v) {
+  atomicMax(m, (unsigned long long)__double_as_longlong(fabs(v)));
+}
+
+__global__ void max_abs_kernel(long long n, const double *__restrict__ v,
+                               unsigned long long *__restrict__ m) {
+  double a = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    a = fmax(a, fabs(v[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+  if ((threadIdx.x & 31) == 0 && a > 0) atomic_max_abs(m, a);
+}
+
+// exponent E with |v| 2^E < 2^bits for every |v| <= m
+__device__ __forceinline__ int scale_exponent(unsigned long long mbits, int bits) {
+  const double m = __longlong_as_double((long long)mbits);
+  if (!(m > 0)) return 0;
+  int e;
+  frexp(m, &e);  // m < 2^e
+  return bits - e;
+}
+
+// Scales of one call (device): out[0..3] the factors of rho, jx, jy, jz;
+// integral the factor of the normalising sums; ex[0..4] the digit
+// exponents of c, c vx, c vy, c vz, W.
+struct TcScales {
+  double out[4];
+  double integral;
+  int ex[5];
+};
+
+__global__ void weight_scale_kernel(const unsigned long long *__restrict__ mbits, double kappa,
+                                    TcScales *sc) {
+  const int e = scale_exponent(mbits[4], 47);
+  sc->ex[4] = e;
+  sc->integral = kappa * ldexp(1.0, -e);
+}
+
+__global__ void charge_scale_kernel(const unsigned long long *__restrict__ mbits, double kappa,
+                                    TcScales *sc) {
+  const int e0 = scale_exponent(mbits[0], 46);
+  sc->ex[0] = e0;
+  sc->out[0] = kappa * ldexp(1.0, -e0);
+  for (int d = 1; d < 4; ++d) {
+    const int e = scale_exponent(mbits[d], 22);
+    sc->ex[d] = e;
+    sc->out[d] = kappa * ldexp(1.0, -e);
+  }
+}
+
+// Position weight digits: W 2^E as a 48-bit integer, six unsigned base-256
+// digits (columns 0-5), a one in column 6 (the indicator sum), per tile row.
+__global__ void weight_digits_kernel(long long tiles, const uint32_t *__restrict__ tile_starts,
+                                     const double *__restrict__ W, const TcScales *sc,
+                                     uint4 *__restrict__ out) {
+  const long long t = blockIdx.x;
+  const int u = threadIdx.x;
+  if (t >= tiles) return;
+  const uint32_t p0 = tile_starts[t];
+  const int npt = (int)(tile_starts[t + 1] - p0);
+  uint32_t w[4] = {0, 0, 0, 0};
+  if (u < npt) {
+    const unsigned long long Wi = (unsigned long long)llrint(ldexp(W[p0 + u], sc->ex[4]));
+    w[0] = (uint32_t)(Wi & 0xffffffffull);
+    w[1] = (uint32_t)((Wi >> 32) & 0xffffull) | (1u << 16);
+  }
+  out[128 * t + u] = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// Per particle (bin order) the deposited charge c and c v: c = q (plain), or
+// q / integral with the integral from the exact sums of the normalisation
+// pass; the scale and hit count feed the statistics.
+template <bool NORM>
+__global__ void charges_kernel(long long n, const uint32_t *__restrict__ n_live,
+                               const double2 *__restrict__ pay,
+                               const unsigned long long *__restrict__ hi,
+                               const unsigned long long *__restrict__ lo,
+                               const uint32_t *__restrict__ hits, const TcScales *sc,
+                               const uint32_t *__restrict__ perm, double *__restrict__ cv,
+                               double *__restrict__ scale_out, double *__restrict__ hits_out,
+                               unsigned long long *__restrict__ mbits, DevStatus *st) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double v[4] = {0, 0, 0, 0};
+  if (k < n) {
+    if (k < (long long)*n_live) {
+      const double q = pay[4 * k + 1].y;
+      const double2 j01 = pay[4 * k + 2], j2 = pay[4 * k + 3];
+      if (NORM) {
+        const double integral =
+            fma((double)hi[k], 1099511627776.0, (double)lo[k]) * sc->integral;
+        if (integral > 0) {
+          const double f = 1.0 / integral;
+          v[0] = q * f;
+          v[1] = j01.x * f;
+          v[2] = j01.y * f;
+          v[3] = j2.x * f;
+        } else {
+          record_warning(st, PRT_WARN_ZERO_MASS, perm ? (long long)perm[k] : k);
+        }
+        scale_out[k] = v[0];
+        hits_out[k] = hits ? (double)hits[k] : 0.0;
+      } else {
+        v[0] = q;
+        v[1] = j01.x;
+        v[2] = j01.y;
+        v[3] = j2.x;
+      }
+    } else if (NORM) {
+      scale_out[k] = 0;
+      hits_out[k] = -1;
+    }
+#pragma unroll
+    for (int d = 0; d < 4; ++d) cv[d * n + k] = v[d];
+  }
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    double a = fabs(v[d]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+    if ((threadIdx.x & 31) == 0 && a > 0) atomic_max_abs(mbits + d, a);
+  }
+}
+
+// Balanced signed base-256 digits (each in [-128, 127]) of X.
+__device__ __forceinline__ void balanced_digits(long long X, int nd, uint8_t *out) {
+  for (int i = 0; i < nd; ++i) {
+    const int d = (int)(int8_t)(uint8_t)(X & 0xff);
+    out[i] = (uint8_t)(int8_t)d;
+    X = (X - d) >> 8;
+  }
+}
+
+// Charge digits per particle (bin order): c 2^E0 in six balanced signed
+// base-256 digits (columns 0-5), each c v component in three (6-8, 9-11,
+// 12-14).
+__global__ void charge_digits_kernel(long long n, const double *__restrict__ cv,
+                                     const TcScales *sc, uint4 *__restrict__ out) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  uint8_t b[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) b[i] = 0;
+  balanced_digits(llrint(ldexp(cv[k], sc->ex[0])), CDIG, b);
+#pragma unroll
+  for (int d = 1; d < 4; ++d)
+    balanced_digits(llrint(ldexp(cv[d * n + k], sc->ex[d])), JDIG, b + CDIG + JDIG * (d - 1));
+  uint32_t w[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    w[i] = (uint32_t)b[4 * i] | ((uint32_t)b[4 * i + 1] << 8) | ((uint32_t)b[4 * i + 2] << 16) |
+           ((uint32_t)b[4 * i + 3] << 24);
+  out[k] = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+template <bool NORM, bool IND>
+int launch_tc(const TcArgs &A, long long tiles, cudaStream_t s) {
+  const int smem = (int)sizeof(Smem);
+  PRT_CHECK_CUDA(cudaFuncSetAttribute(tc_deposit_kernel<NORM, IND>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  tc_deposit_kernel<NORM, IND><<<(unsigned)tiles, THREADS, smem, s>>>(A);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  return PRT_OK;
+}
+
+}  // namespace
+
+int prt_deposit_shape_tc(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
+                         prt_shape_function shape, const double *iw, long long n,
+                         const double *x, const double *q, const double *v,
+                         const uint32_t *el, double *rho, double *j,
+                         prt_deposit_stats *stats, cudaStream_t s) {
+  const PositionSet &PS = mesh->positions;
+  const bool norm = mode == PRT_DEPOSIT_NORMALIZED;
+  int rc;
+  BinGrid G;
+  if (!choose_bins(mesh, mesh->box_lo, mesh->box_hi, shape.radius * BIN_FRACTION, shape.radius,
+                   G, &rc))
+    return rc;
+  const long long tiles = PS.tiles;
+  const double kappa = shape.normalizer * shape.radius * shape.radius /
+                       (4.0 * (double)SIGMA * (double)SIGMA);
+
+  // position operands of the tiles (kept while mesh and radius stay the same)
+  uint4 *tile_ops = (uint4 *)ws_buffer(ws, PRT_WS_TC_TILES, 4096 * (size_t)tiles, &rc);
+  if (!tile_ops) return rc;
+  if (ws->tc_mesh_uid != mesh->uid || ws->tc_radius != shape.radius) {
+    tile_operands_kernel<<<(unsigned)tiles, 128, 0, s>>>(tiles, PS.tile_starts, PS.tile_boxes,
+                                                         PS.pos, 1.0 / shape.radius, tile_ops);
+    PRT_CHECK_CUDA(cudaGetLastError());
+    ws->tc_mesh_uid = mesh->uid;
+    ws->tc_radius = shape.radius;
+  }
+
+  // particles binned, sorted and packed (payload weight q, q v)
+  DepParticles P;
+  {
+    ScopedTimer timer(ws, PRT_TIME_DEPOSIT_STAGE, s);
+    if ((rc = stage_particles(ws, G, n, x, q, v, el, nullptr, 1.0, nullptr, P, s))) return rc;
+  }
+  const uint32_t *perm =
+      (const uint32_t *)ws_buffer(ws, PRT_WS_DEP_VALS, 8 * (size_t)n, &rc) + n;
+
+  // per-particle scratch (bin order)
+  const size_t b_u64 = align256(8 * (size_t)n), b_u32 = align256(4 * (size_t)n);
+  const size_t b_cv = align256(32 * (size_t)n), b_dig = align256(16 * (size_t)n);
+  const size_t b_f64 = align256(8 * (size_t)n);
+  char *part = (char *)ws_buffer(ws, PRT_WS_TC_PART,
+                                 2 * b_u64 + b_u32 + b_cv + b_dig + (norm ? 2 * b_f64 : 0), &rc);
+  if (!part) return rc;
+  unsigned long long *nhi = (unsigned long long *)part;
+  unsigned long long *nlo = (unsigned long long *)(part + b_u64);
+  uint32_t *hits = (uint32_t *)(part + 2 * b_u64);
+  double *cv = (double *)(part + 2 * b_u64 + b_u32);
+  uint4 *cdig = (uint4 *)(part + 2 * b_u64 + b_u32 + b_cv);
+  double *scale_bin = norm ? (double *)(part + 2 * b_u64 + b_u32 + b_cv + b_dig) : nullptr;
+  double *hits_bin = norm ? (double *)(part + 2 * b_u64 + b_u32 + b_cv + b_dig + b_f64) : nullptr;
+
+  // small: maxima of |c|, |c v|, W (bits), the candidate counter, the scales
+  char *misc = (char *)ws_buffer(ws, PRT_WS_TC_MISC, 1024, &rc);
+  if (!misc) return rc;
+  unsigned long long *mbits = (unsigned long long *)misc;  // [8]
+  unsigned long long *counters = mbits + 8;                 // [4]
+  TcScales *sc = (TcScales *)(misc + 256);
+  PRT_CHECK_CUDA(cudaMemsetAsync(misc, 0, 256, s));
+
+  double *vals = (double *)ws_buffer(ws, PRT_WS_DEP_VALUES, 4 * sizeof(double) * PS.count, &rc);
+  if (!vals) return rc;
+
+  TcArgs A;
+  A.G = G;
+  A.pay = reinterpret_cast<const double2 *>(P.payload);
+  A.starts = P.starts;
+  A.tile_starts = PS.tile_starts;
+  A.tile_boxes = PS.tile_boxes;
+  A.tile_ops = tile_ops;
+  A.wdig = nullptr;
+  A.cdig = cdig;
+  A.order = nullptr;
+  A.radius = shape.radius;
+  A.inv_radius = 1.0 / shape.radius;
+  A.norm_hi = nhi;
+  A.norm_lo = nlo;
+  A.hits = hits;
+  A.out_scale = sc->out;
+  A.vals = vals;
+  A.npos = PS.count;
+  A.counters = counters;
+  A.st = ws->status;
+
+  const unsigned pblocks = (unsigned)((n + 255) / 256);
+  const uint32_t *n_live = P.starts + G.nbins;
+  if (norm) {
+    // position weights -> digits; the normalisation pass
+    char *wbuf = (char *)ws_buffer(ws, PRT_WS_TC_WDIG,
+                                   2048 * (size_t)tiles + align256(8 * (size_t)PS.count), &rc);
+    if (!wbuf) return rc;
+    uint4 *wdig = (uint4 *)wbuf;
+    double *W = (double *)(wbuf + 2048 * (size_t)tiles);
+    if ((rc = prt_dep_position_weights(mesh, ws, iw, W, s))) return rc;
+    max_abs_kernel<<<592, 256, 0, s>>>(PS.count, W, mbits + 4);
+    PRT_CHECK_CUDA(cudaGetLastError());
+    weight_scale_kernel<<<1, 1, 0, s>>>(mbits, kappa, sc);
+    PRT_CHECK_CUDA(cudaGetLastError());
+    weight_digits_kernel<<<(unsigned)tiles, 128, 0, s>>>(tiles, PS.tile_starts, W, sc, wdig);
+    PRT_CHECK_CUDA(cudaGetLastError());
+    PRT_CHECK_CUDA(cudaMemsetAsync(part, 0, 2 * b_u64 + b_u32, s));
+    A.wdig = wdig;
+    {
+      ScopedTimer timer(ws, PRT_TIME_DEPOSIT_NORMALIZE, s);
+      rc = stats ? launch_tc<true, true>(A, tiles, s) : launch_tc<true, false>(A, tiles, s);
+      if (rc) return rc;
+    }
+    charges_kernel<true><<<pblocks, 256, 0, s>>>(n, n_live, A.pay, nhi, nlo,
+                                                 stats ? hits : nullptr, sc, perm, cv, scale_bin,
+                                                 hits_bin, mbits, ws->status);
+  } else {
+    charges_kernel<false><<<pblocks, 256, 0, s>>>(n, n_live, A.pay, nullptr, nullptr, nullptr,
+                                                  sc, perm, cv, nullptr, nullptr, mbits,
+                                                  ws->status);
+  }
+  PRT_CHECK_CUDA(cudaGetLastError());
+  charge_scale_kernel<<<1, 1, 0, s>>>(mbits, kappa, sc);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  charge_digits_kernel<<<pblocks, 256, 0, s>>>(n, cv, sc, cdig);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  {
+    ScopedTimer timer(ws, PRT_TIME_DEPOSIT_GATHER, s);
+    if ((rc = launch_tc<false, false>(A, tiles, s))) return rc;
+  }
+  if ((rc = prt_dep_expand(mesh, vals, rho, j, s))) return rc;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    if (norm && (rc = prt_dep_norm_stats(ws, n, scale_bin, hits_bin, stats, s))) return rc;
+    unsigned long long h[2] = {0, 0};
+    PRT_CHECK_CUDA(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, s));
+    PRT_CHECK_CUDA(cudaStreamSynchronize(s));
+    // candidates of the deposition pass (the normalisation pass adds the same)
+    stats->evaluated_pairs = (double)(h[0] / (norm ? 2 : 1)) * TM;
+  }
+  return PRT_OK;
+}

@@ -24,6 +24,10 @@ enum {
   PRT_WS_DIAGNOSTICS,
   PRT_WS_AVERAGE,
   PRT_WS_GROUP_ORDER,
+  PRT_WS_TC_TILES,    // tensor-core deposition: position-tile operands (per radius)
+  PRT_WS_TC_WDIG,     // tensor-core deposition: position weight digits
+  PRT_WS_TC_PART,     // tensor-core deposition: per-particle sums, values and digits
+  PRT_WS_TC_MISC,     // tensor-core deposition: scales, counters, tile order
   PRT_WS_SLOTS
 };
 
@@ -57,6 +61,12 @@ struct PositionSet {
     const double *spheres = nullptr;    // [groups][4], bin order
     const uint32_t *ranges = nullptr;   // [groups][2]: first position, count
   } centre_bins;
+  // tiles of the tensor-core deposition: runs of <= 128 consecutive
+  // positions that never straddle a Morton cell of about PRT_TILE_TARGET
+  // positions, with their bounding boxes
+  long long tiles = 0;
+  const uint32_t *tile_starts = nullptr;  // [tiles + 1]
+  const double *tile_boxes = nullptr;     // [tiles][6]: centre xyz, half extent xyz
 };
 
 struct prt_mesh {
@@ -65,6 +75,7 @@ struct prt_mesh {
   const double *face_radii = nullptr;      // [E][4]
   double box_lo[3], box_hi[3];             // node bounding box of the mesh
   PositionSet positions;
+  unsigned long long uid = 0;              // unique per created mesh (workspace caches)
 };
 
 // CUDA-event timing of the main kernels (prt_workspace_timing).
@@ -80,6 +91,10 @@ struct KernelTimer {
 struct prt_workspace {
   void *buf[PRT_WS_SLOTS];
   size_t cap[PRT_WS_SLOTS];
+  // PRT_WS_TC_TILES holds the tile operands of the mesh with this uid and
+  // this shape radius
+  unsigned long long tc_mesh_uid = 0;
+  double tc_radius = 0;
   DevStatus *status = nullptr;
   bool timing = false;
   KernelTimer timers[PRT_TIME_CATEGORIES];
@@ -123,5 +138,29 @@ constexpr double PRT_GROUP_TARGET = 24.0;
 #define PRT_WIDE_CELL_BITS 1
 #endif
 
+// target positions per Morton cell when cutting the tensor-core tiles
+#ifndef PRT_TILE_TARGET
+#define PRT_TILE_TARGET 128.0
+#endif
+
 void *ws_buffer(prt_workspace *ws, int slot, size_t bytes, int *rc);
 int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d);
+
+// Shared pieces of the shape deposition (deposit.cu) used by the
+// tensor-core form (deposit_tc.cu).
+// W[u] = sum over the nodes at position u of w_i |J_e| (device; iw a HOST [Np]).
+int prt_dep_position_weights(const prt_mesh *mesh, prt_workspace *ws, const double *iw,
+                             double *W, cudaStream_t s);
+// The normalising depositor's statistics from per-particle scales and hit
+// counts (hits < 0: removed particle); synchronises s.
+int prt_dep_norm_stats(prt_workspace *ws, long long n, const double *scale,
+                       const double *hits, prt_deposit_stats *stats, cudaStream_t s);
+// rho/j of every node from the values of its position (vals [4][npos]).
+int prt_dep_expand(const prt_mesh *mesh, const double *vals, double *rho, double *j,
+                   cudaStream_t s);
+// The chosen-form shape deposition on the tensor cores (alpha = 2).
+int prt_deposit_shape_tc(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
+                         prt_shape_function shape, const double *iw, long long n,
+                         const double *x, const double *q, const double *v,
+                         const uint32_t *el, double *rho, double *j,
+                         prt_deposit_stats *stats, cudaStream_t s);

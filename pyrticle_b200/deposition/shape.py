@@ -20,15 +20,20 @@ class NormalizationStats:
         self.el_per_particle_stats = StatsGatherer()
 
 
-PRECISIONS = {"fp64": 0, "mixed": 1}
+PRECISIONS = {"fp64": 0, "mixed": 1, "mixed_simt": 2}
 
 
 class ShapeFunctionDepositor(Depositor):
     """rho[n] = sum_p q_p S(x_n - x_p), j = sum_p q_p v_p S (dep_shape.hpp).
 
-    ``precision="fp64"`` is the plain form; ``"mixed"`` evaluates the shape
-    weights and sums them in FP32 per batch of 32 particles, combining the
-    batches into FP64 per node (the normalising scale stays FP64)."""
+    ``precision="fp64"`` is the plain form. ``"mixed"`` is the chosen form:
+    on the tensor cores, the shape weights from a split-FP16 product rounded
+    to 16-bit integers and summed exactly against 48-bit integer charges
+    (24-bit currents), combined into FP64 per node; the normalising integral
+    is summed exactly from the same weights, so the normalised depositor's
+    deposited charge equals the particles' charge to FP64 rounding.
+    ``"mixed_simt"`` evaluates the weights and sums them in FP32 per batch of
+    32 particles on the CUDA cores, combining the batches into FP64."""
 
     name = "Shape"
     mode = _lib.DEPOSIT_PLAIN
@@ -36,7 +41,7 @@ class ShapeFunctionDepositor(Depositor):
     def __init__(self, precision="fp64"):
         Depositor.__init__(self)
         if precision not in PRECISIONS:
-            raise ValueError("precision must be 'fp64' or 'mixed'")
+            raise ValueError("precision must be 'fp64', 'mixed' or 'mixed_simt'")
         self.precision = precision
 
     def set_shape_function(self, state, sf):
