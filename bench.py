@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--depositor", default="normalized", choices=["normalized", "plain"],
+                    help="NormalizedShapeFunctionDepositor (the chosen form's deposition, "
+                         "default) or ShapeFunctionDepositor")
     ap.add_argument("--adjoint-scale", type=float, default=1.0,
                     help="particle-count scale of the differentiable workload (1M electrons)")
     return ap.parse_args()
@@ -104,15 +107,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_method(w, torch):
+def build_method(w, torch, normalized=False):
     from pyrticle_b200.cloud import PicMethod
-    from pyrticle_b200.deposition.shape import ShapeFunctionDepositor
+    from pyrticle_b200.deposition.shape import (NormalizedShapeFunctionDepositor,
+                                                ShapeFunctionDepositor)
     from pyrticle_b200.discretization import Discretization
     from pyrticle_b200.pusher import MonomialParticlePusher
     from pyrticle_b200.tools import PolynomialShapeFunction
     from pyrticle_b200.units import SIUnitsWithNaturalConstants as U
     discr = Discretization(w.mesh, w.order, nodes=w.nodes)
-    m = PicMethod(discr, U, ShapeFunctionDepositor(), MonomialParticlePusher(), 3, 3)
+    dep = NormalizedShapeFunctionDepositor() if normalized else ShapeFunctionDepositor()
+    m = PicMethod(discr, U, dep, MonomialParticlePusher(), 3, 3)
     sf = PolynomialShapeFunction(w.shape_radius, 3, 2)
     m.depositor.set_shape_function(None, sf)
     return m, sf
@@ -458,7 +463,7 @@ def main():
     from pyrticle_b200.sharding import allreduce_densities, max_over_ranks
 
     w = problems.make(args.workload, scale=args.scale, seed=1 + rank)
-    m, sf = build_method(w, torch)
+    m, sf = build_method(w, torch, normalized=args.depositor == "normalized")
     s = m.make_state()
     m.add_particles_from_arrays(s, w.positions, w.momenta, w.charges, w.masses)
     fields = torch.as_tensor(w.fields, device="cuda")
@@ -492,7 +497,7 @@ def main():
         """K timed steps of one form (device events, max over ranks) with the
         per-category kernel times."""
         _lib.check(m.lib.prt_workspace_timing(m.workspace, 1))
-        for cat in range(4):
+        for cat in range(7):
             timing_read(m, cat, reset=True)
         if world > 1:
             dist.barrier()
@@ -511,7 +516,8 @@ def main():
         if world > 1:
             t = max_over_ranks(t, "cuda")
         kernel = {name: timing_read(m, cat) for cat, name in
-                  enumerate(("deposit_gather", "deposit_stage", "lsrk_stage", "sort"))}
+                  ((0, "deposit_gather"), (1, "deposit_stage"), (2, "lsrk_stage"), (3, "sort"),
+                   (6, "deposit_normalize"))}
         return float(t), kernel
 
     ms64, kernel64 = timed("fp64")

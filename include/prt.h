@@ -279,7 +279,9 @@ int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
 #define PRT_NOALLOC_SCRATCH_BYTES (64u << 20)
 
 /* No counterpart in the reference: the plain-form deposition of
- * prt_deposit_shape (mode PRT_DEPOSIT_PLAIN, FP64) for callers that must not
+ * prt_deposit_shape (mode PRT_DEPOSIT_PLAIN, FP64; the same sums in another
+ * order, so the results agree to rounding, about 1e-15 relative, not
+ * bitwise) for callers that must not
  * allocate device memory while they run -- code with a fixed, pre-reserved
  * memory budget, real-time loops where an allocation would stall or
  * synchronise the device, or hosts that forbid it. It calls no cudaMalloc,
@@ -289,7 +291,10 @@ int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
  * caller's, as for prt_deposit_shape; rho or j may be NULL.
  *  - The first call on a device looks up the array's device address
  *    (cudaGetSymbolAddress) and caches it; make that first call before any
- *    stream capture.
+ *    stream capture. The cache lives as long as the process: after a
+ *    cudaDeviceReset the address is stale, so do not call this entry point
+ *    on a device that was reset.
+ *  - With rho and j both NULL the call does nothing.
  *  - A call whose scratch (about 84 bytes per particle + 32 bytes per
  *    distinct node position + bins + radix-sort storage) exceeds the
  *    capacity returns PRT_ERR_CAPACITY before touching any pointer.

@@ -37,6 +37,7 @@ TIME_LSRK_STAGE = 2
 TIME_SORT = 3
 TIME_STAGE_ADJOINT = 4
 TIME_DEPOSIT_ADJOINT = 5
+TIME_DEPOSIT_NORMALIZE = 6
 MAX_FIELD_BASIS = 4
 BEAM_MOMENTS = 25
 BM = dict(count=0, charge=1, p=2, ke=5, ke2=6, x=7, x2=10, xp=13, xp2=16, xxp=19, qv=22)

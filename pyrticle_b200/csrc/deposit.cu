@@ -13,16 +13,23 @@
 // positions, which needs no floating-point atomics and is deterministic:
 //
 //   1. set-up (host, once per mesh): merge coincident nodes into positions,
-//      order them along a Morton curve; 32 consecutive positions form a warp
-//      group (bounding sphere), 128 a CTA tile (bounding box);
+//      order them along a Morton curve, cut the order into warp groups
+//      (<= 32 positions at Morton cells of ~24) and wide groups (<= 64, two
+//      positions per lane), each with its bounding sphere;
 //   2. per call: bin the particles (bin width radius/2), radix sort by bin,
-//      pack a 64-byte payload per particle in bin order;
-//   3. one CTA per tile: stream the particles of the bin rows within the
-//      radius of the tile box through shared memory; each warp compacts the
-//      particles inside its sphere grown by the radius into its own buffer
-//      and all 32 lanes walk that buffer (one position per lane), with a
-//      branchless weight; rho, j accumulate in registers in bin order;
+//      pack a 64-byte payload per particle in bin order; estimate each
+//      group's work (the particles of its bin rows) and launch the groups
+//      heaviest first;
+//   3. one warp per group, warps independent: the warp streams the
+//      particles of the bin rows within the radius of its box straight from
+//      L2, culls them against the box grown by the radius, appends the
+//      survivors to a private shared-memory ring (ballot), and every 32
+//      entries the lanes walk the batch with a branch-free weight, two
+//      positions per lane; rho, j accumulate in a fixed order;
 //   4. expand: every node takes its position's values.
+//
+// The chosen form's tensor-core deposition (deposit_tc.cu) shares steps 1,
+// 2 and 4 and replaces step 3.
 //
 // Periodic axes use particle images shifted by the period, the images the
 // walk uses when it crosses a periodic face.
@@ -1314,7 +1321,9 @@ void *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
 std::mutex g_noalloc_mutex;
 
 // Device address of the scratch for the current device; looked up with
-// cudaGetSymbolAddress on the first call per device and cached.
+// cudaGetSymbolAddress on the first call per device and cached for the life
+// of the process (a cudaDeviceReset, which tears down the context that owns
+// the array, leaves the cached address stale).
 int noalloc_scratch_address(void **out) {
   int dev = 0;
   PRT_CHECK_CUDA(cudaGetDevice(&dev));
@@ -1363,6 +1372,7 @@ extern "C" int prt_deposit_shape_noalloc(const prt_mesh *mesh, prt_shape_functio
   if (need > (size_t)PRT_NOALLOC_SCRATCH_BYTES) return PRT_ERR_CAPACITY;
   if (n > 0 && (!x || !q || (j && !v))) return PRT_ERR_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;
+  if (!rho && !j) return PRT_OK;  // nothing requested: no work
   if (n == 0) {
     if (rho) PRT_CHECK_CUDA(cudaMemsetAsync(rho, 0, nn * sizeof(double), s));
     if (j) PRT_CHECK_CUDA(cudaMemsetAsync(j, 0, 3 * nn * sizeof(double), s));

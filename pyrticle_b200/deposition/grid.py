@@ -299,7 +299,7 @@ def orthonormal_vandermonde_fast(points, modes):
     return refelement.orthonormal_vandermonde(points, modes)
 
 
-def average_groups(mesh, nodes, nodes_per_element, chunk=200000):
+def average_groups(mesh, nodes, nodes_per_element, chunk=None):
     """The continuity groups of prepare_average_groups (grid.py:143-183): the
     DG nodes that face pairs identify, merged into connected sets. For every
     interior face (periodic ones included: positions compared modulo the
@@ -320,6 +320,8 @@ def average_groups(mesh, nodes, nodes_per_element, chunk=200000):
     inval = np.iinfo(np.uint32).max
     e_idx, f_idx = np.nonzero((nb != inval) & (nb > np.arange(E)[:, None]))
     per = mesh.periodicity_max - mesh.periodicity_min
+    # face pairs per chunk: the [F, Np, Np, 3] differences stay near 160 MB
+    chunk = chunk or max(1, int(2e7) // (Np * Np))
     rows, cols = [], []
     for c0 in range(0, len(e_idx), chunk):
         e1 = e_idx[c0:c0 + chunk]

@@ -1,4 +1,4 @@
-"""Particle files (cloud.py:606-671 as files; SURVEY's checkpoint/resume):
+"""Particle files (cloud.py:606-671 as files; checkpoint and resume):
 VTK output round trip on the host; checkpoint save/load of the device store
 with removed particles, then identical steps from the saved and the
 restored state."""
