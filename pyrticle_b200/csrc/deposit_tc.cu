@@ -929,6 +929,32 @@ __global__ void charge_digits_kernel(long long n, const double *__restrict__ cv,
   out[k] = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
+// Work estimate per tile: the particles in the bin rows of its box grown by
+// the radius (periodic images ignored), keyed for a descending sort so that
+// the heaviest tiles start first and the light ones fill the tail of the
+// launch. Each tile is one CTA whatever the order, so no result changes.
+__global__ void tile_work_kernel(long long tiles, const double *__restrict__ tile_boxes,
+                                 BinGrid G, const uint32_t *__restrict__ starts, double radius,
+                                 uint32_t *__restrict__ work, uint32_t *__restrict__ ids) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= tiles) return;
+  int lo[3], hi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double c = tile_boxes[6 * t + d], h = tile_boxes[6 * t + 3 + d] + radius;
+    lo[d] = max(0, min(G.dims[d] - 1, bin_floor(G, d, c - h)));
+    hi[d] = max(0, min(G.dims[d] - 1, bin_floor(G, d, c + h)));
+  }
+  unsigned long long wsum = 0;
+  for (int bz = lo[2]; bz <= hi[2]; ++bz)
+    for (int by = lo[1]; by <= hi[1]; ++by) {
+      const long long row = (long long)G.dims[0] * (by + (long long)G.dims[1] * bz);
+      wsum += starts[row + hi[0] + 1] - starts[row + lo[0]];
+    }
+  work[t] = (uint32_t)min(wsum, 0xffffffffull);
+  ids[t] = (uint32_t)t;
+}
+
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 template <bool NORM, bool IND>
@@ -994,8 +1020,9 @@ int prt_deposit_shape_tc(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
   double *scale_bin = norm ? (double *)(part + 2 * b_u64 + b_u32 + b_cv + b_dig) : nullptr;
   double *hits_bin = norm ? (double *)(part + 2 * b_u64 + b_u32 + b_cv + b_dig + b_f64) : nullptr;
 
-  // small: maxima of |c|, |c v|, W (bits), the candidate counter, the scales
-  char *misc = (char *)ws_buffer(ws, PRT_WS_TC_MISC, 1024, &rc);
+  // small: maxima of |c|, |c v|, W (bits), the candidate counter, the
+  // scales; then the tiles' launch order (heaviest first)
+  char *misc = (char *)ws_buffer(ws, PRT_WS_TC_MISC, 1024 + 16 * (size_t)tiles, &rc);
   if (!misc) return rc;
   unsigned long long *mbits = (unsigned long long *)misc;  // [8]
   unsigned long long *counters = mbits + 8;                 // [4]
@@ -1015,6 +1042,21 @@ int prt_deposit_shape_tc(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
   A.wdig = nullptr;
   A.cdig = cdig;
   A.order = nullptr;
+  if (tiles > 1) {
+    uint32_t *wk = (uint32_t *)(misc + 1024), *ids = wk + tiles, *wk_out = wk + 2 * tiles,
+             *ids_out = wk + 3 * tiles;
+    tile_work_kernel<<<prt_grid_blocks(tiles, 256), 256, 0, s>>>(tiles, PS.tile_boxes, G,
+                                                                 P.starts, shape.radius, wk, ids);
+    PRT_CHECK_CUDA(cudaGetLastError());
+    size_t tb = 0;
+    PRT_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, wk, wk_out, ids,
+                                                             ids_out, (int)tiles, 0, 32, s));
+    void *tmp = ws_buffer(ws, PRT_WS_CUB, tb, &rc);
+    if (!tmp) return rc;
+    PRT_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tb, wk, wk_out, ids, ids_out,
+                                                             (int)tiles, 0, 32, s));
+    A.order = ids_out;
+  }
   A.radius = shape.radius;
   A.inv_radius = 1.0 / shape.radius;
   A.norm_hi = nhi;
