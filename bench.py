@@ -125,18 +125,24 @@ def build_method(w, torch, normalized=False):
 
 def count_pairs(m, state, sf):
     """Exact (particle, position) and (particle, node) pair counts inside the
-    radius (one extra deposition call)."""
+    radius, the pairs the FP64 kernel evaluates after its culls, and the
+    pairs the tensor-core kernel evaluates per pass (candidates x 128 tile
+    rows); two extra deposition calls."""
     from pyrticle_b200 import _lib
     import torch
     nn = len(m.discretization)
     rho = torch.empty((nn,), dtype=torch.float64, device="cuda")
-    st = _lib.DepositStats()
-    _lib.check(m.lib.prt_deposit_shape(
-        m.mesh_data.handle, m.workspace, _lib.DEPOSIT_PLAIN,
-        _lib.ShapeFunctionDesc(sf.radius, sf.exponent, sf.normalizer), None, len(state),
-        state.x.data_ptr(), state.q.data_ptr(), None, state.el.data_ptr(), rho.data_ptr(),
-        None, 0, C.byref(st), C.c_void_p(torch.cuda.current_stream().cuda_stream)))
-    return int(st.pair_count), int(st.node_pair_count), int(st.evaluated_pairs)
+    out = []
+    for prec in (0, 1):
+        st = _lib.DepositStats()
+        _lib.check(m.lib.prt_deposit_shape(
+            m.mesh_data.handle, m.workspace, _lib.DEPOSIT_PLAIN,
+            _lib.ShapeFunctionDesc(sf.radius, sf.exponent, sf.normalizer), None, len(state),
+            state.x.data_ptr(), state.q.data_ptr(), None, state.el.data_ptr(), rho.data_ptr(),
+            None, prec, C.byref(st), C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        out.append(st)
+    return (int(out[0].pair_count), int(out[0].node_pair_count), int(out[0].evaluated_pairs),
+            int(out[1].evaluated_pairs))
 
 
 def timing_read(m, cat, reset=True):
@@ -487,7 +493,7 @@ def main():
         for _ in range(args.warmup):
             one_step(form)
     torch.cuda.synchronize()
-    pairs, node_pairs, evaluated = count_pairs(m, s, sf)
+    pairs, node_pairs, evaluated, evaluated_tc = count_pairs(m, s, sf)
     accuracy = form_accuracy(m, s, fields, w.dt, torch)
 
     clocks = ClockSampler(local)
@@ -619,11 +625,20 @@ def main():
     peaks, src = measured_peaks()
     fp64 = fp64_peak_tflops(torch)
     fp32 = fp32_peak_tflops(torch)
-    # dominant kernel of each form: the deposition gather, 15 flops per
-    # (particle, distinct position) pair within the radius
+    bf16 = float(peaks.get("bf16_tflops", 1590.0))
+    # chosen form: the tensor-core deposition (tc_deposit_kernel), two passes
+    # of the same tile kernel: the normalising integrals, then the deposition
     gms, gk = kernel["deposit_gather"]
     avg_gather = gms / max(gk, 1)
-    achieved = 15.0 * pairs / (avg_gather * 1e-3) / 1e12
+    nms, nk = kernel["deposit_normalize"]
+    avg_norm = nms / max(nk, 1)
+    # executed tensor work per evaluated (position, particle) pair in dense
+    # FP16 equivalents: the score, 2 x 16 (kind::f16, K = 16); the sums,
+    # 2 weight digits x 16 columns x 2 int8 ops counted at half (the int8
+    # rate is twice the FP16 rate)
+    tensor_per_pair = 32 + 32
+    achieved = tensor_per_pair * evaluated_tc / (avg_gather * 1e-3) / 1e12
+    useful = 15.0 * pairs / (avg_gather * 1e-3) / 1e12
     gms64, gk64 = kernel64["deposit_gather"]
     avg_gather64 = gms64 / max(gk64, 1)
     achieved64 = 15.0 * pairs / (avg_gather64 * 1e-3) / 1e12
@@ -633,26 +648,28 @@ def main():
                    f"radius per launch ({node_pairs} (particle, node) pairs over all DG nodes; "
                    f"coincident nodes are evaluated once; {evaluated} pairs evaluated after "
                    f"culling)")
-    roofline = {"bound": "fp32", "kernel": "deposit_groups_mixed_kernel (deposition, chosen form)",
-                "achieved": achieved, "peak": fp32, "unit": "TFLOP/s", "frac": achieved / fp32,
+    roofline = {"bound": "tensor",
+                "kernel": "tc_deposit_kernel (deposition pass, chosen form)",
+                "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
                 "traffic": None,
-                "traffic_note": "null: the deposition is FP32-pipe bound and its DRAM traffic "
-                                "does not grow in proportion to the particles (the rho/j "
-                                "output is per node); ncu at 1.6M particles on the same mesh "
-                                "measured 434 MB per launch (241 MB read, 193 MB write), "
-                                "under 1% of DRAM peak",
-                "peak_source": "cuBLAS SGEMM 8192^3 (TF32 off) measured in this run (FP32 "
-                               "pipe; MEASURED_PEAKS.json has no FP32 figure)",
-                "algorithmic": algorithmic + f"; {avg_gather:.3f} ms per launch",
+                "peak_source": ("MEASURED_PEAKS.json bf16_tflops" if src == "measured" else
+                                "fallback 1,590 TFLOP/s (dense BF16, this pool)"),
+                "algorithmic": (f"{tensor_per_pair} dense-FP16-equivalent tensor flops per "
+                                f"evaluated (position, particle) pair x {evaluated_tc} evaluated "
+                                f"pairs per launch (128 tile rows x candidates); {pairs} pairs "
+                                f"within the radius; {avg_gather:.3f} ms per launch"),
+                "evaluated_per_useful_pair": evaluated_tc / max(pairs, 1),
+                "useful_pairs_per_s": pairs / (avg_gather * 1e-3),
+                "useful_fp32_equivalent": {
+                    "achieved": useful, "peak": fp32, "unit": "TFLOP/s", "frac": useful / fp32,
+                    "note": "15 flops per pair within the radius against the FP32 CUDA-core "
+                            "rate (cuBLAS SGEMM, TF32 off, measured in this run): the work "
+                            "the CUDA-core form of this deposition does per pair"},
+                "normalize_pass_ms": avg_norm,
                 "secondary": {"bound": "hbm", "kernel": "lsrk_stage_mixed_kernel<3>",
                               "achieved": stage_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                               "frac": stage_gbs / peaks["hbm_gbs"],
                               "algorithmic": "216 B per particle per stage",
-                              "traffic": 443.869184e6 / 1.6e6 * n,
-                              "traffic_note": "ncu at 1.6M particles (444 MB per launch), "
-                                              "scaled by the particle count: 277 B per "
-                                              "particle against 216 algorithmic (element "
-                                              "gathers re-read from DRAM)",
                               "peak_source": src}}
     fp64_block = {
         "value": value64, "unit": METRIC, "ms_per_step": ms64 / args.steps,
@@ -662,34 +679,46 @@ def main():
                      "frac": achieved64 / fp64, "traffic": None,
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
                      "algorithmic": algorithmic + f"; {avg_gather64:.3f} ms per launch"},
-        "form": "plain form: FP64 throughout"}
+        "form": ("plain form: FP64 throughout" +
+                 ("; NormalizedShapeFunctionDepositor: FP64 integral and scale per particle"
+                  if args.depositor == "normalized" else ""))}
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64 (mixed: FP32 deposition, split-BF16 tensor-core Lagrange "
-                     "values, FP64 state/force/locate/combine)",
+            "dtype": "f16/i8 tensor + f32 + f64 (mixed: split-FP16 tensor-core shape scores, "
+                     "16-bit integer weights summed exactly on the int8 tensor cores, FP64 "
+                     "per-node combine and normalisation; split-BF16 tensor-core Lagrange "
+                     "values; FP64 state/force/locate)",
             "data": "synthetic (seeded mesh, particles and fields of the workload)",
             "config": {"workload": f"{args.workload}: {w.mesh.element_count} tets order "
                                    f"{w.order}, {n} particles/GPU, shape radius "
-                                   f"{w.shape_radius * 100:g} cm, chosen (mixed) form",
+                                   f"{w.shape_radius * 100:g} cm, chosen (mixed) form, "
+                                   f"{'Normalized' if args.depositor == 'normalized' else ''}"
+                                   f"ShapeFunctionDepositor",
                        "particles_per_gpu": n, "elements": w.mesh.element_count,
                        "nodes": nn, "order": w.order, "form": "mixed",
+                       "depositor": args.depositor,
                        "l2": f"inputs larger than L2 ({216 * n / 1e9:.1f} GB particle state per stage)",
                        "parallelism": f"particles sharded over {world} GPU(s), NCCL "
                                       "all-reduce of rho/j" if world > 1 else "1 GPU"},
             "clocks": clk, "gpu_launches": None, "roofline": roofline,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kernel.items()},
             "pairs_per_deposition": {"positions": pairs, "nodes": node_pairs,
-                                     "evaluated": evaluated},
+                                     "evaluated_fp64_kernel": evaluated,
+                                     "evaluated_tensor_core_kernel": evaluated_tc},
             "fp64": fp64_block, "speedup_mixed_vs_fp64": ms64 / ms,
             "accuracy_mixed_vs_fp64": accuracy}
     # libprt's own kernels in the timed region of the headline form (CUB's
     # radix-sort kernels not counted): per sort iota + 5 permutation gathers
-    # (x, p, q, m, ids; the residuals are dead at a step boundary);
-    # per RK stage one fused kernel; per deposition bin keys, bin starts,
-    # payload, the group work estimate, the gather and the expansion to nodes.
-    line["gpu_launches"] = int(kernel["lsrk_stage"][1] + 3 * kernel["deposit_gather"][1] +
-                               3 * kernel["deposit_stage"][1] + 6 * kernel["sort"][1])
+    # (x, p, q, m, ids; the residuals are dead at a step boundary); per RK
+    # stage one fused kernel; per deposition bin keys, bin starts, payload,
+    # the tile work estimate, charges, charge scale, charge digits, the
+    # deposition pass and the expansion to nodes (9), and with the
+    # normalising depositor position weights, their maximum, scale and
+    # digits, the normalisation pass and the two statistics kernels (7).
+    per_dep = 9 + (7 if args.depositor == "normalized" else 0)
+    line["gpu_launches"] = int(kernel["lsrk_stage"][1] + per_dep * kernel["deposit_gather"][1] +
+                               6 * kernel["sort"][1])
     if e2e:
         line["e2e"] = e2e
     if not args.no_adjoint and world == 1:

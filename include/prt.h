@@ -308,6 +308,43 @@ int prt_deposit_shape_noalloc(const prt_mesh *mesh, prt_shape_function shape,
                               const uint32_t *elements, double *rho, double *j,
                               void *stream);
 
+/* Sharded form of the chosen-form deposition (PRT_PRECISION_MIXED, shape
+ * exponent 2) for one process per GPU. No reference counterpart: the
+ * reference is a single process; its deposition is a sum over particles
+ * (dep_target.hpp:203-273), which these three steps split by particle. Every
+ * rank holds the mesh and deposits its own particles:
+ *  1. prt_deposit_shape_charges: bins the rank's particles and, in the
+ *     normalising mode, integrates each one's shape over all node positions
+ *     (the mesh is replicated, so this needs no exchange); writes the maxima
+ *     of |c|, |c vx|, |c vy|, |c vz| over the rank's particles to
+ *     `local_max` (device, [4]); c = q (plain) or q / integral;
+ *  -- the caller all-reduces the four maxima with MAX --
+ *  2. prt_deposit_shape_sums: the deposition pass with the digits scaled by
+ *     the global maxima, writing per distinct node position the 16 digit
+ *     sums (device [16][npos], npos from prt_mesh_position_count); every
+ *     value is an integer below 2^45 held in an FP64;
+ *  -- the caller all-reduces the sums with SUM: integers below 2^53 add
+ *     exactly in any order --
+ *  3. prt_deposit_shape_combine: rho [Nn] and j [3][Nn] (either may be NULL)
+ *     from the summed digit sums and the global maxima.
+ * rho and j are then bitwise the same for any number of ranks and any split
+ * of the particles, and equal to prt_deposit_shape's with every particle on
+ * one GPU. Steps 1 and 2 share workspace state: call them with the same
+ * workspace, mesh, shape and n, with no other deposition in between.
+ * `stats` (step 1, may be NULL) as prt_deposit_shape's, for the rank's
+ * particles; it synchronises `stream`. */
+int prt_mesh_position_count(const prt_mesh *mesh, int64_t *count);
+int prt_deposit_shape_charges(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
+                              prt_shape_function shape, const double *integral_weights,
+                              int64_t n, const double *positions, const double *charges,
+                              const double *velocities, const uint32_t *elements,
+                              double *local_max, prt_deposit_stats *stats, void *stream);
+int prt_deposit_shape_sums(const prt_mesh *mesh, prt_workspace *ws, prt_shape_function shape,
+                           int64_t n, const double *global_max, double *sums, void *stream);
+int prt_deposit_shape_combine(const prt_mesh *mesh, prt_workspace *ws,
+                              prt_shape_function shape, const double *global_max,
+                              const double *sums, double *rho, double *j, void *stream);
+
 /* ------------------------------------------------------------ grid dep --- */
 
 /* One brick (grid.hpp:159-340): cell-centred points origin + (idx + 1/2) h,

@@ -152,6 +152,12 @@ SIGNATURES = {
                                  _vp, _vp, _vp, _vp, _i32, C.POINTER(DepositStats), _vp]),
     "prt_deposit_shape_noalloc": (_i32, [_vp, ShapeFunctionDesc, _i64, _vp, _vp, _vp, _vp,
                                          _vp, _vp, _vp]),
+    "prt_mesh_position_count": (_i32, [_vp, C.POINTER(_i64)]),
+    "prt_deposit_shape_charges": (_i32, [_vp, _vp, _i32, ShapeFunctionDesc, _dp, _i64, _vp,
+                                         _vp, _vp, _vp, _vp, C.POINTER(DepositStats), _vp]),
+    "prt_deposit_shape_sums": (_i32, [_vp, _vp, ShapeFunctionDesc, _i64, _vp, _vp, _vp]),
+    "prt_deposit_shape_combine": (_i32, [_vp, _vp, ShapeFunctionDesc, _vp, _vp, _vp, _vp,
+                                         _vp]),
     "prt_grid_create": (_i32, [_vp, C.POINTER(GridDesc), C.POINTER(_vp)]),
     "prt_grid_destroy": (_i32, [_vp]),
     "prt_deposit_grid": (_i32, [_vp, _vp, _i32, ShapeFunctionDesc, _i64, _vp, _vp, _vp,

@@ -144,7 +144,7 @@ extern "C" int prt_mesh_destroy(prt_mesh *m) {
                         P.pos, P.node_to_pos, P.run_starts, P.run_nodes,
                         P.group_starts, P.group_spheres,
                         P.centre_bins.starts, P.centre_bins.spheres, P.centre_bins.ranges,
-                        P.wide_starts, P.wide_spheres, P.tile_starts, P.tile_boxes};
+                        P.wide_starts, P.wide_spheres};
   for (const void *p : ptrs)
     if (p) cudaFree((void *)p);
   delete m;

@@ -910,6 +910,11 @@ int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
   run_starts.push_back((uint32_t)nn);
   PositionSet &P = m->positions;
   P.count = npos;
+  // host copies for the tensor-core tiles, which are cut per shape radius
+  m->pos_host = pos;
+  m->pos_key.resize(npos);
+  for (long long u = 0; u < npos; ++u) m->pos_key[u] = key[order[run_starts[u]]];
+  m->morton_ext = ext;
   int rc;
   if ((rc = upload_vec(pos, &P.pos))) return rc;
   if ((rc = upload_vec(node_to_pos, &P.node_to_pos))) return rc;
@@ -975,40 +980,7 @@ int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
     if ((rc = upload_vec(gstart, &P.group_starts))) return rc;
     if ((rc = upload_vec(spheres, &P.group_spheres))) return rc;
 
-    // tensor-core tiles: runs of <= 128 positions cut at Morton cells of
-    // about PRT_TILE_TARGET positions, with bounding boxes
-    {
-      const double tside = std::cbrt(PRT_TILE_TARGET * vol / std::max<long long>(1, npos));
-      int tlevel = (int)std::lround(std::log2(ext / tside));
-      tlevel = std::min(std::max(tlevel, 0), 21);
-      const int tshift = 3 * (21 - tlevel);
-      std::vector<uint32_t> ts;
-      ts.reserve(npos / 64 + 2);
-      uint64_t prev_cell = ~0ull;
-      for (long long u = 0; u < npos; ++u) {
-        const uint64_t cell = key[order[run_starts[u]]] >> tshift;
-        if (u == 0 || cell != prev_cell || u - ts.back() >= 128) ts.push_back((uint32_t)u);
-        prev_cell = cell;
-      }
-      ts.push_back((uint32_t)npos);
-      const long long nt = (long long)ts.size() - 1;
-      std::vector<double> tb(6 * (size_t)std::max<long long>(1, nt), 0.0);
-      for (long long t = 0; t < nt; ++t) {
-        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (uint32_t p = ts[t]; p < ts[t + 1]; ++p)
-          for (int a = 0; a < 3; ++a) {
-            lo[a] = std::min(lo[a], pos[3 * p + a]);
-            hi[a] = std::max(hi[a], pos[3 * p + a]);
-          }
-        for (int a = 0; a < 3; ++a) {
-          tb[6 * t + a] = 0.5 * (lo[a] + hi[a]);
-          tb[6 * t + 3 + a] = 0.5 * (hi[a] - lo[a]);
-        }
-      }
-      P.tiles = nt;
-      if ((rc = upload_vec(ts, &P.tile_starts))) return rc;
-      if ((rc = upload_vec(tb, &P.tile_boxes))) return rc;
-    }
+
 
     // centre bins: width about the mean group radius
     auto &CB = P.centre_bins;
@@ -1169,15 +1141,18 @@ extern "C" int prt_deposit_shape(const prt_mesh *mesh, prt_workspace *ws, int32_
     PRT_CHECK_CUDA(cudaGetLastError());
     const CentreBinsDev CB = centre_bins_dev(PS);
     const unsigned nblk = (unsigned)((n + 32 * NORM_WARPS - 1) / (32 * NORM_WARPS));
-    if (a2)
-      normalize_kernel<true><<<nblk, 32 * NORM_WARPS, 0, s>>>(
-          mesh->dev, CB, PS.pos, PS.count, W, S, shape.normalizer, n, x, q, el, sc, sc + n,
-          ws->status);
-    else
-      normalize_kernel<false><<<nblk, 32 * NORM_WARPS, 0, s>>>(
-          mesh->dev, CB, PS.pos, PS.count, W, S, shape.normalizer, n, x, q, el, sc, sc + n,
-          ws->status);
-    PRT_CHECK_CUDA(cudaGetLastError());
+    {
+      ScopedTimer norm_timer(ws, PRT_TIME_DEPOSIT_NORMALIZE, s);
+      if (a2)
+        normalize_kernel<true><<<nblk, 32 * NORM_WARPS, 0, s>>>(
+            mesh->dev, CB, PS.pos, PS.count, W, S, shape.normalizer, n, x, q, el, sc, sc + n,
+            ws->status);
+      else
+        normalize_kernel<false><<<nblk, 32 * NORM_WARPS, 0, s>>>(
+            mesh->dev, CB, PS.pos, PS.count, W, S, shape.normalizer, n, x, q, el, sc, sc + n,
+            ws->status);
+      PRT_CHECK_CUDA(cudaGetLastError());
+    }
     if (stats) {
       const long long need = (n + 255) / 256;
       const int sb = (int)(need < STATS_BLOCKS ? need : STATS_BLOCKS);

@@ -8,7 +8,8 @@
 // pairs within the radius a of S(r) = N (a - r^2/a)^2 = N a^2 (1 - r^2/a^2)^2.
 //
 // Here the distinct node positions are cut into tiles of <= 128 (Morton
-// runs, PositionSet::tiles) and each CTA takes one tile:
+// runs within cells at most two radii wide, cut per shape radius) and each
+// CTA takes one tile:
 //
 //  1. candidates: the particles of the bin rows within the radius of the
 //     tile's box (particles binned and packed in bin order, binning.cuh),
@@ -24,28 +25,32 @@
 //     accumulate in FP32 into tensor memory;
 //  3. weight: each thread reads its position's row (tcgen05.ld), forms
 //     t = s + |s| = 2 max(s, 0) and the integer F = round(t^2) =
-//     round(4 SIGMA^2 max(1 - r^2/a^2, 0)^2) <= 65525 with one FMA
+//     round(4 SIGMA^2 max(1 - r^2/a^2, 0)^2) < 2^23 with one FMA
 //     (t t + 2^23 puts the rounded integer in the low mantissa bits), and
-//     stores its two bytes as unsigned 8-bit digits in shared memory;
+//     stores its three bytes as unsigned 8-bit digits in shared memory;
 //  4. sums: tcgen05.mma kind::i8 (int32 accumulation in tensor memory,
 //     exact) of the weight digits against
-//      - deposition: per candidate the charge c (q or q / integral) as a
-//        48-bit integer in six balanced signed digits and c v (each
-//        component 24 bits, three digits), one 16-column operand; rows =
+//      - deposition: per candidate the charge c (q or q / integral) scaled
+//        to a signed integer below 2^46 in six balanced signed digits and
+//        c v (each component below 2^22, three digits), one 16-column
+//        operand; rows =
 //        positions, so tensor memory accumulates sum_p F c per position over
 //        the whole tile (folded into FP64 every 256 chunks before int32
 //        could overflow);
-//      - normalisation: per position the weight sum_{nodes} |J_e| w_i as a
-//        48-bit integer in six unsigned digits; the weight digits are read
+//      - normalisation: per position the weight sum_{nodes} |J_e| w_i (which
+//        is negative at some nodes of order 2 and 4 elements) as a 47-bit
+//        signed integer in six balanced signed digits; the weight digits are read
 //        transposed (MN-major: the same bytes are rows = candidates), so the
 //        product is, per candidate, sum_u F W over the tile, which the CTA
 //        adds to the particle's integral as two exact 64-bit integer atomics
-//        (high and low part): integer sums do not depend on the order, so the
-//        result is deterministic.
+//        (signed high part, low 40 bits): integer sums do not depend on the
+//        order, so the result is deterministic.
 //     The weights F of both passes are bitwise the same (same tiles, same
 //     operands, same instructions), and every sum of F is exact, so the
-//     deposited charge sum_u W_u rho_u equals sum_p q_p up to the 48-bit
+//     deposited charge sum_u W_u rho_u equals sum_p q_p up to the 46-bit
 //     representation of W and c and the final FP64 roundings (~1e-16).
+//     The tiles are at most two radii wide, so every score operand stays
+//     within FP16 range.
 //
 // Synchronisation per chunk k of a CTA: the score MMA of chunk k runs while
 // the warps stage chunk k+1; the weights of chunk k are written once the
@@ -57,8 +62,10 @@
 #include <cuda_fp16.h>
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "binning.cuh"
 
@@ -72,19 +79,21 @@ constexpr int RING = 512;        // candidate slots in shared memory
 constexpr int THREADS = 256;     // eight warps
 constexpr int MAXSEG = 512;      // bin-row segments per tile
 constexpr uint32_t TMEM_COLS = 256;
-constexpr uint32_t COL_ACC = 128;  // accumulators: high digit +0, low digit +16, indicator +32
-constexpr float SIGMA = 127.99f;   // 4 SIGMA^2 < 65536
+constexpr uint32_t COL_ACC = 128;  // accumulators: weight digit d at +16 d, indicator at +48
+constexpr int FDIG = 3;            // weight digits (bytes 2, 1, 0 of the weight)
+constexpr float SIGMA = 1448.0f;   // 4 SIGMA^2 < 2^23
 constexpr unsigned SPIN = 1u << 22;  // try_wait rounds before a wait gives up
 constexpr int FLUSH_CHUNKS = 256;    // int32 accumulation window (256 * 128 * 255 * 128 < 2^31)
 constexpr int CDIG = 6, JDIG = 3, WDIG = 6;
+
 
 struct Smem {
   uint8_t apos[2 * TM * 16];     // position operand, K-major: [K chunk][row][16 B]
   uint8_t bcand[2 * RING * 16];  // candidate operands, K-major: [K chunk][slot][16 B]
   uint8_t bdig[RING * 16];       // charge digits per slot (16 columns, MN-major)
   uint8_t wdig[TM * 16];         // weight digits per position (16 columns, MN-major)
-  // weight digits: [high, low, indicator][16-candidate block][position][16 B]
-  uint8_t fdig[3][NC / 16][TM][16];
+  // weight digits: [byte 2, byte 1, byte 0, indicator][16-candidate block][position][16 B]
+  uint8_t fdig[FDIG + 1][NC / 16][TM][16];
   uint32_t slot_id[RING];        // bin-order particle of a slot (normalisation)
   uint32_t seg_start[MAXSEG];    // first bin-order particle of a segment
   uint32_t seg_pref[MAXSEG + 1]; // stream offset of a segment
@@ -101,7 +110,7 @@ struct TcArgs {
   const double2 *__restrict__ pay;      // [n][4] bin-order payload (x, y | z, q | ...)
   const uint32_t *__restrict__ starts;  // [nbins + 1]
   const uint32_t *__restrict__ tile_starts;
-  const double *__restrict__ tile_boxes;
+  const double *__restrict__ tile_boxes; // [tiles][6]: centre xyz, half extent xyz
   const uint4 *__restrict__ tile_ops;   // [tiles][256] position operands
   const uint4 *__restrict__ wdig;       // [tiles][128] weight digits
   const uint4 *__restrict__ cdig;       // [n] charge digits, bin order
@@ -111,6 +120,7 @@ struct TcArgs {
   uint32_t *__restrict__ hits;                                      // [n], bin order
   const double *__restrict__ out_scale;  // [4]: rho, jx, jy, jz factors
   double *__restrict__ vals;             // [4][npos]
+  double *__restrict__ sums;             // [16][npos] digit sums instead of vals (or NULL)
   long long npos;
   unsigned long long *__restrict__ counters;  // [0]: candidates over all tiles
   DevStatus *st;
@@ -200,6 +210,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
         "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t addr, uint32_t (&r)[8]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7])
       : "r"(addr)
       : "memory");
 }
@@ -453,7 +472,7 @@ __device__ __forceinline__ void weights(Smem &S, uint32_t tmem, int warp, int la
     tmem_wait_ld();
 #pragma unroll
     for (int g = 0; g < 2; ++g) {
-      uint32_t lo[4], hi[4], ind[4];
+      uint32_t b0[4], b1[4], b2[4], ind[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         uint32_t b[4];
@@ -464,15 +483,18 @@ __device__ __forceinline__ void weights(Smem &S, uint32_t tmem, int warp, int la
           b[e] = __float_as_uint(fmaf(t, t, 8388608.0f));  // 2^23 + round(t^2)
         }
         const uint32_t x = prmt(b[0], b[1], 0x5140), y = prmt(b[2], b[3], 0x5140);
-        lo[j] = prmt(x, y, 0x5410);  // byte 0 of each value
-        hi[j] = prmt(x, y, 0x7632);  // byte 1 of each value
-        if (IND) ind[j] = __vcmpne4(lo[j] | hi[j], 0u) & 0x01010101u;
+        const uint32_t z = prmt(b[0], b[1], 0x0062), w = prmt(b[2], b[3], 0x0062);
+        b0[j] = prmt(x, y, 0x5410);  // byte 0 of each value
+        b1[j] = prmt(x, y, 0x7632);  // byte 1
+        b2[j] = prmt(z, w, 0x5410);  // byte 2
+        if (IND) ind[j] = __vcmpne4(b0[j] | b1[j] | b2[j], 0u) & 0x01010101u;
       }
       const int blk = (64 * h + 32 * half + 16 * g) >> 4;
-      *reinterpret_cast<uint4 *>(&S.fdig[0][blk][row][0]) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-      *reinterpret_cast<uint4 *>(&S.fdig[1][blk][row][0]) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+      *reinterpret_cast<uint4 *>(&S.fdig[0][blk][row][0]) = make_uint4(b2[0], b2[1], b2[2], b2[3]);
+      *reinterpret_cast<uint4 *>(&S.fdig[1][blk][row][0]) = make_uint4(b1[0], b1[1], b1[2], b1[3]);
+      *reinterpret_cast<uint4 *>(&S.fdig[2][blk][row][0]) = make_uint4(b0[0], b0[1], b0[2], b0[3]);
       if (IND)
-        *reinterpret_cast<uint4 *>(&S.fdig[2][blk][row][0]) =
+        *reinterpret_cast<uint4 *>(&S.fdig[FDIG][blk][row][0]) =
             make_uint4(ind[0], ind[1], ind[2], ind[3]);
     }
   }
@@ -486,8 +508,28 @@ constexpr uint32_t IDESC_SCORE =
 //  MN-major (charge digits), N = 16
 constexpr uint32_t IDESC_DEP = (2u << 4) | (1u << 10) | (1u << 16) | (2u << 17) | (8u << 24);
 //  normalisation sums: D S32, A U8 MN-major (weights read as rows =
-//  candidates), B U8 MN-major (position weight digits), N = 16
-constexpr uint32_t IDESC_NORM = (2u << 4) | (1u << 15) | (1u << 16) | (2u << 17) | (8u << 24);
+//  candidates), B S8 MN-major (position weight digits), N = 16
+constexpr uint32_t IDESC_NORM =
+    (2u << 4) | (1u << 10) | (1u << 15) | (1u << 16) | (2u << 17) | (8u << 24);
+
+// rho, j of a position from its digit sums T (T_i = sum_p F c_i over the
+// particles, c_i the i-th digit column): charge = sum_i T_i 256^i over the
+// six charge digits, each current component over its three, times the
+// output scales. One formula for the fused epilogue and for the combination
+// of summed partial results, so both give the same bits.
+__device__ __forceinline__ void combine_position(const double T[16],
+                                                 const double *__restrict__ scale,
+                                                 double out[4]) {
+  double r = T[CDIG - 1];
+#pragma unroll
+  for (int i = CDIG - 2; i >= 0; --i) r = fma(r, 256.0, T[i]);
+  out[0] = r * scale[0];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int b = CDIG + JDIG * d;
+    out[1 + d] = fma(fma(T[b + 2], 256.0, T[b + 1]), 256.0, T[b]) * scale[1 + d];
+  }
+}
 
 template <bool NORM, bool IND>
 __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
@@ -540,11 +582,12 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   const uint32_t a_pos = smem_u32(S.apos), b_cand = smem_u32(S.bcand), b_dig = smem_u32(S.bdig);
   const uint32_t w_dig = smem_u32(S.wdig), f_dig = smem_u32(S.fdig);
 
-  // per thread: position row 32 (warp % 4) + lane, digit warp / 4 of the
-  // deposition's accumulators (FP64 across int32 windows)
-  double acc[16];
+  // per thread: position row 32 (warp % 4) + lane, digit columns
+  // 8 (warp / 4) .. + 7 of the deposition's sums over the weight digits
+  // (FP64, exact integers, across int32 windows)
+  double acc[8];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) acc[i] = 0;
+  for (int i = 0; i < 8; ++i) acc[i] = 0;
 
   bool ok = S.abort == 0;
   int issued_s = 0, issued_a = 0, waited_s = 0, waited_a = 0;
@@ -553,34 +596,45 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   // readout of a normalisation chunk: per candidate its sum over the tile
   auto norm_readout = [&](int chunk, int nvalid) {
     if (warp < 4) {
-      uint32_t d1[16], d0[16], di[16];
+      uint32_t d2[8], d1[8], d0[8], di[8];
       const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
-      tmem_ld16(lane_addr + COL_ACC, d1);
-      tmem_ld16(lane_addr + COL_ACC + 16, d0);
-      if (IND) tmem_ld16(lane_addr + COL_ACC + 32, di);
+      tmem_ld8(lane_addr + COL_ACC, d2);
+      tmem_ld8(lane_addr + COL_ACC + 16, d1);
+      tmem_ld8(lane_addr + COL_ACC + 32, d0);
+      if (IND) tmem_ld8(lane_addr + COL_ACC + 48, di);
       tmem_wait_ld();
       const int cr = 32 * warp + lane;
       if (cr < nvalid) {
-        unsigned __int128 P = 0;
+        // the tile's part of the integral, exactly:
+        // sum_kk 256^kk (65536 D2 + 256 D1 + D0)
+        __int128 P = 0;
 #pragma unroll
         for (int kk = 0; kk < WDIG; ++kk)
-          P += ((unsigned __int128)d1[kk] << (8 * kk + 8)) + ((unsigned __int128)d0[kk] << (8 * kk));
+          P += ((__int128)(int)d2[kk] << (8 * kk + 16)) + ((__int128)(int)d1[kk] << (8 * kk + 8)) +
+               ((__int128)(int)d0[kk] << (8 * kk));
         const uint32_t id = S.slot_id[(chunk * NC + cr) & (RING - 1)];
         if (P != 0) {
-          atomicAdd(A.norm_hi + id, (unsigned long long)(P >> 40));
-          atomicAdd(A.norm_lo + id, (unsigned long long)(P & ((1ull << 40) - 1)));
+          // P = H 2^40 + L, 0 <= L < 2^40: both parts add exactly (H modulo 2^64)
+          const __int128 H = P >> 40;
+          atomicAdd(A.norm_hi + id, (unsigned long long)(long long)H);
+          atomicAdd(A.norm_lo + id, (unsigned long long)(P - (H << 40)));
         }
         if (IND && di[WDIG]) atomicAdd(A.hits + id, di[WDIG]);
       }
     }
   };
-  // deposition accumulators -> FP64
+  // deposition accumulators -> FP64: per digit column the exact integer
+  // 65536 D2 + 256 D1 + D0 (below 2^53)
   auto dep_fold = [&]() {
-    uint32_t d[16];
-    tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + COL_ACC + 16 * (warp >> 2), d);
+    uint32_t d2[8], d1[8], d0[8];
+    const uint32_t base = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + COL_ACC + 8 * (warp >> 2);
+    tmem_ld8(base, d2);
+    tmem_ld8(base + 16, d1);
+    tmem_ld8(base + 32, d0);
     tmem_wait_ld();
 #pragma unroll
-    for (int i = 0; i < 16; ++i) acc[i] += (double)(int)d[i];
+    for (int i = 0; i < 8; ++i)
+      acc[i] += (double)(65536ll * (int)d2[i] + 256ll * (int)d1[i] + (int)d0[i]);
   };
   auto wait_s = [&]() {
     const bool w = mbar_wait(bar_s, (uint32_t)(waited_s & 1));
@@ -645,7 +699,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
       const int slot0 = (k * NC) & (RING - 1);
       if (NORM) {
 #pragma unroll
-        for (int d = 0; d < (IND ? 3 : 2); ++d)
+        for (int d = 0; d < (IND ? FDIG + 1 : FDIG); ++d)
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj)
             mma_i8(tmem + COL_ACC + 16 * d,
@@ -653,7 +707,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
                    sdesc(w_dig + jj * 512, 128, 128), IDESC_NORM, jj > 0);
       } else {
 #pragma unroll
-        for (int d = 0; d < 2; ++d)
+        for (int d = 0; d < FDIG; ++d)
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj)
             mma_i8(tmem + COL_ACC + 16 * d,
@@ -700,33 +754,27 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   } else {
     if (tid == 0) atomicAdd(A.counters, (unsigned long long)S.tail);
     if (!NORM) {
-      // per position: T_i = 256 (high-digit sum) + (low-digit sum), then the
-      // charge (six digits) and current (three digits per component)
-      double(*lo_acc)[16] = reinterpret_cast<double(*)[16]>(&S.fdig[0][0][0][0]);
+      // per position the 16 digit sums T_i (exact integers), then the charge
+      // (six digits) and current (three digits per component)
+      double(*tsum)[16] = reinterpret_cast<double(*)[16]>(&S.fdig[0][0][0][0]);
       const int row = 32 * (warp & 3) + lane;
-      if (warp >= 4) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) lo_acc[row][i] = acc[i];
-      }
+      for (int i = 0; i < 8; ++i) tsum[row][8 * (warp >> 2) + i] = acc[i];
       __syncthreads();
       if (warp < 4 && row < npt) {
         double T[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) T[i] = fma(256.0, acc[i], lo_acc[row][i]);
-        double r = T[CDIG - 1];
-#pragma unroll
-        for (int i = CDIG - 2; i >= 0; --i) r = fma(r, 256.0, T[i]);
-        double jc[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const int b = CDIG + JDIG * d;
-          jc[d] = fma(fma(T[b + 2], 256.0, T[b + 1]), 256.0, T[b]);
-        }
+        for (int i = 0; i < 16; ++i) T[i] = tsum[row][i];
         const long long u = p0 + row;
-        A.vals[u] = r * A.out_scale[0];
-        A.vals[A.npos + u] = jc[0] * A.out_scale[1];
-        A.vals[2 * A.npos + u] = jc[1] * A.out_scale[2];
-        A.vals[3 * A.npos + u] = jc[2] * A.out_scale[3];
+        if (A.sums) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) A.sums[i * A.npos + u] = T[i];
+        } else {
+          double o[4];
+          combine_position(T, A.out_scale, o);
+#pragma unroll
+          for (int d = 0; d < 4; ++d) A.vals[d * A.npos + u] = o[d];
+        }
       }
     }
   }
@@ -808,11 +856,13 @@ struct TcScales {
 
 __global__ void weight_scale_kernel(const unsigned long long *__restrict__ mbits, double kappa,
                                     TcScales *sc) {
-  const int e = scale_exponent(mbits[4], 47);
+  const int e = scale_exponent(mbits[4], 46);
   sc->ex[4] = e;
   sc->integral = kappa * ldexp(1.0, -e);
 }
 
+// (the maxima are given as the bit patterns of non-negative doubles, which
+// order like the doubles themselves)
 __global__ void charge_scale_kernel(const unsigned long long *__restrict__ mbits, double kappa,
                                     TcScales *sc) {
   const int e0 = scale_exponent(mbits[0], 46);
@@ -825,8 +875,27 @@ __global__ void charge_scale_kernel(const unsigned long long *__restrict__ mbits
   }
 }
 
-// Position weight digits: W 2^E as a 48-bit integer, six unsigned base-256
-// digits (columns 0-5), a one in column 6 (the indicator sum), per tile row.
+// Balanced signed base-256 digits (each in [-128, 127]) of X.
+__device__ __forceinline__ void balanced_digits(long long X, int nd, uint8_t *out) {
+  for (int i = 0; i < nd; ++i) {
+    const int d = (int)(int8_t)(uint8_t)(X & 0xff);
+    out[i] = (uint8_t)(int8_t)d;
+    X = (X - d) >> 8;
+  }
+}
+
+__device__ __forceinline__ uint4 pack16(const uint8_t b[16]) {
+  uint32_t w[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    w[i] = (uint32_t)b[4 * i] | ((uint32_t)b[4 * i + 1] << 8) | ((uint32_t)b[4 * i + 2] << 16) |
+           ((uint32_t)b[4 * i + 3] << 24);
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// Position weight digits: W 2^E (|W 2^E| < 2^46) in six balanced signed
+// base-256 digits (columns 0-5), a one in column 6 (the indicator sum), per
+// tile row.
 __global__ void weight_digits_kernel(long long tiles, const uint32_t *__restrict__ tile_starts,
                                      const double *__restrict__ W, const TcScales *sc,
                                      uint4 *__restrict__ out) {
@@ -835,13 +904,14 @@ __global__ void weight_digits_kernel(long long tiles, const uint32_t *__restrict
   if (t >= tiles) return;
   const uint32_t p0 = tile_starts[t];
   const int npt = (int)(tile_starts[t + 1] - p0);
-  uint32_t w[4] = {0, 0, 0, 0};
+  uint8_t b[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) b[i] = 0;
   if (u < npt) {
-    const unsigned long long Wi = (unsigned long long)llrint(ldexp(W[p0 + u], sc->ex[4]));
-    w[0] = (uint32_t)(Wi & 0xffffffffull);
-    w[1] = (uint32_t)((Wi >> 32) & 0xffffull) | (1u << 16);
+    balanced_digits(llrint(ldexp(W[p0 + u], sc->ex[4])), WDIG, b);
+    b[WDIG] = 1;
   }
-  out[128 * t + u] = make_uint4(w[0], w[1], w[2], w[3]);
+  out[128 * t + u] = pack16(b);
 }
 
 // Per particle (bin order) the deposited charge c and c v: c = q (plain), or
@@ -864,8 +934,8 @@ __global__ void charges_kernel(long long n, const uint32_t *__restrict__ n_live,
       const double2 j01 = pay[4 * k + 2], j2 = pay[4 * k + 3];
       if (NORM) {
         const double integral =
-            fma((double)hi[k], 1099511627776.0, (double)lo[k]) * sc->integral;
-        if (integral > 0) {
+            fma((double)(long long)hi[k], 1099511627776.0, (double)lo[k]) * sc->integral;
+        if (integral != 0) {
           const double f = 1.0 / integral;
           v[0] = q * f;
           v[1] = j01.x * f;
@@ -898,15 +968,6 @@ __global__ void charges_kernel(long long n, const uint32_t *__restrict__ n_live,
   }
 }
 
-// Balanced signed base-256 digits (each in [-128, 127]) of X.
-__device__ __forceinline__ void balanced_digits(long long X, int nd, uint8_t *out) {
-  for (int i = 0; i < nd; ++i) {
-    const int d = (int)(int8_t)(uint8_t)(X & 0xff);
-    out[i] = (uint8_t)(int8_t)d;
-    X = (X - d) >> 8;
-  }
-}
-
 // Charge digits per particle (bin order): c 2^E0 in six balanced signed
 // base-256 digits (columns 0-5), each c v component in three (6-8, 9-11,
 // 12-14).
@@ -921,12 +982,7 @@ __global__ void charge_digits_kernel(long long n, const double *__restrict__ cv,
 #pragma unroll
   for (int d = 1; d < 4; ++d)
     balanced_digits(llrint(ldexp(cv[d * n + k], sc->ex[d])), JDIG, b + CDIG + JDIG * (d - 1));
-  uint32_t w[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-    w[i] = (uint32_t)b[4 * i] | ((uint32_t)b[4 * i + 1] << 8) | ((uint32_t)b[4 * i + 2] << 16) |
-           ((uint32_t)b[4 * i + 3] << 24);
-  out[k] = make_uint4(w[0], w[1], w[2], w[3]);
+  out[k] = pack16(b);
 }
 
 // Work estimate per tile: the particles in the bin rows of its box grown by
@@ -957,6 +1013,19 @@ __global__ void tile_work_kernel(long long tiles, const double *__restrict__ til
 
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// rho, j of every position from summed digit sums (sharded form, step 3)
+__global__ void combine_kernel(long long npos, const double *__restrict__ sums,
+                               const TcScales *sc, double *__restrict__ vals) {
+  const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (u >= npos) return;
+  double T[16], o[4];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) T[i] = sums[i * npos + u];
+  combine_position(T, sc->out, o);
+#pragma unroll
+  for (int d = 0; d < 4; ++d) vals[d * npos + u] = o[d];
+}
+
 template <bool NORM, bool IND>
 int launch_tc(const TcArgs &A, long long tiles, cudaStream_t s) {
   const int smem = (int)sizeof(Smem);
@@ -967,85 +1036,191 @@ int launch_tc(const TcArgs &A, long long tiles, cudaStream_t s) {
   return PRT_OK;
 }
 
-}  // namespace
+// The workspace buffers of a call with n particles (the same sizes give the
+// same buffers, so the steps of the sharded form find them again).
+struct TcPtrs {
+  unsigned long long *nhi, *nlo;
+  uint32_t *hits;
+  double *cv;
+  uint4 *cdig;
+  double *scale_bin, *hits_bin;
+  unsigned long long *mbits, *counters;
+  TcScales *sc;
+  uint32_t *order_buf;
+  uint4 *tile_ops;
+  const uint32_t *tile_starts;
+  const double *tile_boxes;
+  double *vals;
+  const uint32_t *perm;
+};
 
-int prt_deposit_shape_tc(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
-                         prt_shape_function shape, const double *iw, long long n,
-                         const double *x, const double *q, const double *v,
-                         const uint32_t *el, double *rho, double *j,
-                         prt_deposit_stats *stats, cudaStream_t s) {
+// The tiles of a mesh for a shape radius, kept in the workspace while mesh
+// and radius stay the same: runs of <= 128 consecutive positions (Morton
+// order) within Morton cells of about PRT_TILE_TARGET positions and at most
+// two radii wide (so that a candidate lies within 2 radii of the tile centre
+// along every axis and the score operands stay in FP16 range), with their
+// bounding boxes and the position operands.
+int tc_tiles(const prt_mesh *mesh, prt_workspace *ws, double radius, cudaStream_t s) {
+  if (ws->tc_mesh_uid == mesh->uid && ws->tc_radius == radius && ws->tc_tiles > 0)
+    return PRT_OK;
   const PositionSet &PS = mesh->positions;
-  const bool norm = mode == PRT_DEPOSIT_NORMALIZED;
+  const long long npos = PS.count;
+  const double ext = mesh->morton_ext;
+  double vol = 1;
+  for (int a = 0; a < 3; ++a) vol *= std::max(mesh->box_hi[a] - mesh->box_lo[a], 1e-300);
+  const double tside = std::cbrt(PRT_TILE_TARGET * vol / std::max<long long>(1, npos));
+  int lt = (int)std::lround(std::log2(ext / tside));
+  int la = (int)std::ceil(std::log2(ext / (2.0 * radius)) + 1e-9);
+  const int level = std::min(std::max(std::max(lt, la), 0), 21);
+  const int shift = 3 * (21 - level);
+  std::vector<uint32_t> ts;
+  ts.reserve(npos / 64 + 2);
+  uint64_t prev = ~0ull;
+  for (long long u = 0; u < npos; ++u) {
+    const uint64_t cell = mesh->pos_key[u] >> shift;
+    if (u == 0 || cell != prev || u - ts.back() >= TM) ts.push_back((uint32_t)u);
+    prev = cell;
+  }
+  ts.push_back((uint32_t)npos);
+  const long long nt = (long long)ts.size() - 1;
+  std::vector<double> tb(6 * (size_t)std::max<long long>(1, nt), 0.0);
+  const double *P = mesh->pos_host.data();
+  for (long long t = 0; t < nt; ++t) {
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t u = ts[t]; u < ts[t + 1]; ++u)
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], P[3 * (size_t)u + a]);
+        hi[a] = std::max(hi[a], P[3 * (size_t)u + a]);
+      }
+    for (int a = 0; a < 3; ++a) {
+      tb[6 * t + a] = 0.5 * (lo[a] + hi[a]);
+      tb[6 * t + 3 + a] = 0.5 * (hi[a] - lo[a]);
+    }
+  }
   int rc;
-  BinGrid G;
+  const size_t b_ts = align256(4 * (size_t)(nt + 1));
+  char *set = (char *)ws_buffer(ws, PRT_WS_TC_TILESET, b_ts + 48 * (size_t)nt, &rc);
+  if (!set) return rc;
+  uint4 *ops = (uint4 *)ws_buffer(ws, PRT_WS_TC_TILES, 4096 * (size_t)nt, &rc);
+  if (!ops) return rc;
+  // pageable sources: the copies are staged before the calls return
+  PRT_CHECK_CUDA(cudaMemcpyAsync(set, ts.data(), 4 * (size_t)(nt + 1), cudaMemcpyHostToDevice, s));
+  PRT_CHECK_CUDA(cudaMemcpyAsync(set + b_ts, tb.data(), 48 * (size_t)nt, cudaMemcpyHostToDevice, s));
+  tile_operands_kernel<<<(unsigned)nt, 128, 0, s>>>(nt, (const uint32_t *)set,
+                                                    (const double *)(set + b_ts), PS.pos,
+                                                    1.0 / radius, ops);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  PRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  ws->tc_mesh_uid = mesh->uid;
+  ws->tc_radius = radius;
+  ws->tc_tiles = nt;
+  return PRT_OK;
+}
+
+int tc_buffers(const prt_mesh *mesh, prt_workspace *ws, long long n, TcPtrs &B) {
+  const PositionSet &PS = mesh->positions;
+  const long long tiles = ws->tc_tiles;
+  int rc;
+  const size_t b_u64 = align256(8 * (size_t)n), b_u32 = align256(4 * (size_t)n);
+  const size_t b_cv = align256(32 * (size_t)n), b_dig = align256(16 * (size_t)n);
+  const size_t b_f64 = align256(8 * (size_t)n);
+  char *part = (char *)ws_buffer(ws, PRT_WS_TC_PART,
+                                 2 * b_u64 + b_u32 + b_cv + b_dig + 2 * b_f64, &rc);
+  if (!part) return rc;
+  B.nhi = (unsigned long long *)part;
+  B.nlo = (unsigned long long *)(part + b_u64);
+  B.hits = (uint32_t *)(part + 2 * b_u64);
+  B.cv = (double *)(part + 2 * b_u64 + b_u32);
+  B.cdig = (uint4 *)(part + 2 * b_u64 + b_u32 + b_cv);
+  B.scale_bin = (double *)(part + 2 * b_u64 + b_u32 + b_cv + b_dig);
+  B.hits_bin = (double *)(part + 2 * b_u64 + b_u32 + b_cv + b_dig + b_f64);
+  // small: maxima of |c|, |c v|, W (bits), the candidate counter, the
+  // scales; then the tiles' launch order (heaviest first)
+  char *misc = (char *)ws_buffer(ws, PRT_WS_TC_MISC, 1024 + 16 * (size_t)tiles, &rc);
+  if (!misc) return rc;
+  B.mbits = (unsigned long long *)misc;  // [8]
+  B.counters = B.mbits + 8;             // [4]
+  B.sc = (TcScales *)(misc + 256);
+  B.order_buf = (uint32_t *)(misc + 1024);
+  B.tile_ops = (uint4 *)ws_buffer(ws, PRT_WS_TC_TILES, 4096 * (size_t)tiles, &rc);
+  if (!B.tile_ops) return rc;
+  const size_t b_ts = align256(4 * (size_t)(tiles + 1));
+  char *set = (char *)ws_buffer(ws, PRT_WS_TC_TILESET, b_ts + 48 * (size_t)tiles, &rc);
+  if (!set) return rc;
+  B.tile_starts = (const uint32_t *)set;
+  B.tile_boxes = (const double *)(set + b_ts);
+  B.vals = (double *)ws_buffer(ws, PRT_WS_DEP_VALUES, 4 * sizeof(double) * PS.count, &rc);
+  if (!B.vals) return rc;
+  B.perm = (const uint32_t *)ws_buffer(ws, PRT_WS_DEP_VALS, 8 * (size_t)n, &rc);
+  if (!B.perm) return rc;
+  B.perm += n;  // the second half: bin order -> particle index
+  return PRT_OK;
+}
+
+int tc_bins(const prt_mesh *mesh, prt_shape_function shape, BinGrid &G) {
+  int rc;
   if (!choose_bins(mesh, mesh->box_lo, mesh->box_hi, shape.radius * BIN_FRACTION, shape.radius,
                    G, &rc))
     return rc;
-  const long long tiles = PS.tiles;
-  const double kappa = shape.normalizer * shape.radius * shape.radius /
-                       (4.0 * (double)SIGMA * (double)SIGMA);
+  return PRT_OK;
+}
 
-  // position operands of the tiles (kept while mesh and radius stay the same)
-  uint4 *tile_ops = (uint4 *)ws_buffer(ws, PRT_WS_TC_TILES, 4096 * (size_t)tiles, &rc);
-  if (!tile_ops) return rc;
-  if (ws->tc_mesh_uid != mesh->uid || ws->tc_radius != shape.radius) {
-    tile_operands_kernel<<<(unsigned)tiles, 128, 0, s>>>(tiles, PS.tile_starts, PS.tile_boxes,
-                                                         PS.pos, 1.0 / shape.radius, tile_ops);
-    PRT_CHECK_CUDA(cudaGetLastError());
-    ws->tc_mesh_uid = mesh->uid;
-    ws->tc_radius = shape.radius;
-  }
+double tc_kappa(prt_shape_function shape) {
+  return shape.normalizer * shape.radius * shape.radius / (4.0 * (double)SIGMA * (double)SIGMA);
+}
 
+void tc_args(const prt_mesh *mesh, prt_workspace *ws, prt_shape_function shape,
+             const BinGrid &G, const TcPtrs &B, TcArgs &A) {
+  const PositionSet &PS = mesh->positions;
+  A.G = G;
+  A.pay = reinterpret_cast<const double2 *>(ws->buf[PRT_WS_DEP_PARTICLES]);
+  A.starts = reinterpret_cast<const uint32_t *>(ws->buf[PRT_WS_DEP_BINSTARTS]);
+  A.tile_starts = B.tile_starts;
+  A.tile_boxes = B.tile_boxes;
+  A.tile_ops = B.tile_ops;
+  A.wdig = nullptr;
+  A.cdig = B.cdig;
+  A.order = ws->tc_tiles > 1 ? B.order_buf + 3 * ws->tc_tiles : nullptr;
+  A.radius = shape.radius;
+  A.inv_radius = 1.0 / shape.radius;
+  A.norm_hi = B.nhi;
+  A.norm_lo = B.nlo;
+  A.hits = B.hits;
+  A.out_scale = B.sc->out;
+  A.vals = B.vals;
+  A.sums = nullptr;
+  A.npos = PS.count;
+  A.counters = B.counters;
+  A.st = ws->status;
+}
+
+// Steps 1-2 of a call: tile operands, particles binned and packed, the
+// tiles' launch order, the normalising pass (normalising mode), the
+// deposited charge c and c v per particle and their maxima (B.mbits[0..3]).
+int tc_charges(const prt_mesh *mesh, prt_workspace *ws, int32_t mode, prt_shape_function shape,
+               const double *iw, long long n, const double *x, const double *q, const double *v,
+               const uint32_t *el, bool want_hits, cudaStream_t s, TcPtrs &B, BinGrid &G) {
+  const PositionSet &PS = mesh->positions;
+  const bool norm = mode == PRT_DEPOSIT_NORMALIZED;
+  int rc;
+  if ((rc = tc_bins(mesh, shape, G))) return rc;
+  if ((rc = tc_tiles(mesh, ws, shape.radius, s))) return rc;
+  const long long tiles = ws->tc_tiles;
+  if ((rc = tc_buffers(mesh, ws, n, B))) return rc;
+  const double kappa = tc_kappa(shape);
   // particles binned, sorted and packed (payload weight q, q v)
   DepParticles P;
   {
     ScopedTimer timer(ws, PRT_TIME_DEPOSIT_STAGE, s);
     if ((rc = stage_particles(ws, G, n, x, q, v, el, nullptr, 1.0, nullptr, P, s))) return rc;
   }
-  const uint32_t *perm =
-      (const uint32_t *)ws_buffer(ws, PRT_WS_DEP_VALS, 8 * (size_t)n, &rc) + n;
-
-  // per-particle scratch (bin order)
-  const size_t b_u64 = align256(8 * (size_t)n), b_u32 = align256(4 * (size_t)n);
-  const size_t b_cv = align256(32 * (size_t)n), b_dig = align256(16 * (size_t)n);
-  const size_t b_f64 = align256(8 * (size_t)n);
-  char *part = (char *)ws_buffer(ws, PRT_WS_TC_PART,
-                                 2 * b_u64 + b_u32 + b_cv + b_dig + (norm ? 2 * b_f64 : 0), &rc);
-  if (!part) return rc;
-  unsigned long long *nhi = (unsigned long long *)part;
-  unsigned long long *nlo = (unsigned long long *)(part + b_u64);
-  uint32_t *hits = (uint32_t *)(part + 2 * b_u64);
-  double *cv = (double *)(part + 2 * b_u64 + b_u32);
-  uint4 *cdig = (uint4 *)(part + 2 * b_u64 + b_u32 + b_cv);
-  double *scale_bin = norm ? (double *)(part + 2 * b_u64 + b_u32 + b_cv + b_dig) : nullptr;
-  double *hits_bin = norm ? (double *)(part + 2 * b_u64 + b_u32 + b_cv + b_dig + b_f64) : nullptr;
-
-  // small: maxima of |c|, |c v|, W (bits), the candidate counter, the
-  // scales; then the tiles' launch order (heaviest first)
-  char *misc = (char *)ws_buffer(ws, PRT_WS_TC_MISC, 1024 + 16 * (size_t)tiles, &rc);
-  if (!misc) return rc;
-  unsigned long long *mbits = (unsigned long long *)misc;  // [8]
-  unsigned long long *counters = mbits + 8;                 // [4]
-  TcScales *sc = (TcScales *)(misc + 256);
-  PRT_CHECK_CUDA(cudaMemsetAsync(misc, 0, 256, s));
-
-  double *vals = (double *)ws_buffer(ws, PRT_WS_DEP_VALUES, 4 * sizeof(double) * PS.count, &rc);
-  if (!vals) return rc;
-
-  TcArgs A;
-  A.G = G;
-  A.pay = reinterpret_cast<const double2 *>(P.payload);
-  A.starts = P.starts;
-  A.tile_starts = PS.tile_starts;
-  A.tile_boxes = PS.tile_boxes;
-  A.tile_ops = tile_ops;
-  A.wdig = nullptr;
-  A.cdig = cdig;
-  A.order = nullptr;
+  // buffers may have moved while staging grew the workspace
+  if ((rc = tc_buffers(mesh, ws, n, B))) return rc;
+  PRT_CHECK_CUDA(cudaMemsetAsync(B.mbits, 0, 256, s));
   if (tiles > 1) {
-    uint32_t *wk = (uint32_t *)(misc + 1024), *ids = wk + tiles, *wk_out = wk + 2 * tiles,
+    uint32_t *wk = B.order_buf, *ids = wk + tiles, *wk_out = wk + 2 * tiles,
              *ids_out = wk + 3 * tiles;
-    tile_work_kernel<<<prt_grid_blocks(tiles, 256), 256, 0, s>>>(tiles, PS.tile_boxes, G,
+    tile_work_kernel<<<prt_grid_blocks(tiles, 256), 256, 0, s>>>(tiles, B.tile_boxes, G,
                                                                  P.starts, shape.radius, wk, ids);
     PRT_CHECK_CUDA(cudaGetLastError());
     size_t tb = 0;
@@ -1055,19 +1230,9 @@ int prt_deposit_shape_tc(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
     if (!tmp) return rc;
     PRT_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tb, wk, wk_out, ids, ids_out,
                                                              (int)tiles, 0, 32, s));
-    A.order = ids_out;
   }
-  A.radius = shape.radius;
-  A.inv_radius = 1.0 / shape.radius;
-  A.norm_hi = nhi;
-  A.norm_lo = nlo;
-  A.hits = hits;
-  A.out_scale = sc->out;
-  A.vals = vals;
-  A.npos = PS.count;
-  A.counters = counters;
-  A.st = ws->status;
-
+  TcArgs A;
+  tc_args(mesh, ws, shape, G, B, A);
   const unsigned pblocks = (unsigned)((n + 255) / 256);
   const uint32_t *n_live = P.starts + G.nbins;
   if (norm) {
@@ -1078,45 +1243,146 @@ int prt_deposit_shape_tc(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
     uint4 *wdig = (uint4 *)wbuf;
     double *W = (double *)(wbuf + 2048 * (size_t)tiles);
     if ((rc = prt_dep_position_weights(mesh, ws, iw, W, s))) return rc;
-    max_abs_kernel<<<592, 256, 0, s>>>(PS.count, W, mbits + 4);
+    max_abs_kernel<<<592, 256, 0, s>>>(PS.count, W, B.mbits + 4);
     PRT_CHECK_CUDA(cudaGetLastError());
-    weight_scale_kernel<<<1, 1, 0, s>>>(mbits, kappa, sc);
+    weight_scale_kernel<<<1, 1, 0, s>>>(B.mbits, kappa, B.sc);
     PRT_CHECK_CUDA(cudaGetLastError());
-    weight_digits_kernel<<<(unsigned)tiles, 128, 0, s>>>(tiles, PS.tile_starts, W, sc, wdig);
+    weight_digits_kernel<<<(unsigned)tiles, 128, 0, s>>>(tiles, B.tile_starts, W, B.sc, wdig);
     PRT_CHECK_CUDA(cudaGetLastError());
-    PRT_CHECK_CUDA(cudaMemsetAsync(part, 0, 2 * b_u64 + b_u32, s));
+    PRT_CHECK_CUDA(cudaMemsetAsync(B.nhi, 0, 8 * (size_t)n, s));
+    PRT_CHECK_CUDA(cudaMemsetAsync(B.nlo, 0, 8 * (size_t)n, s));
+    PRT_CHECK_CUDA(cudaMemsetAsync(B.hits, 0, 4 * (size_t)n, s));
     A.wdig = wdig;
     {
       ScopedTimer timer(ws, PRT_TIME_DEPOSIT_NORMALIZE, s);
-      rc = stats ? launch_tc<true, true>(A, tiles, s) : launch_tc<true, false>(A, tiles, s);
+      rc = want_hits ? launch_tc<true, true>(A, tiles, s) : launch_tc<true, false>(A, tiles, s);
       if (rc) return rc;
     }
-    charges_kernel<true><<<pblocks, 256, 0, s>>>(n, n_live, A.pay, nhi, nlo,
-                                                 stats ? hits : nullptr, sc, perm, cv, scale_bin,
-                                                 hits_bin, mbits, ws->status);
+    charges_kernel<true><<<pblocks, 256, 0, s>>>(n, n_live, A.pay, B.nhi, B.nlo,
+                                                 want_hits ? B.hits : nullptr, B.sc, B.perm, B.cv,
+                                                 B.scale_bin, B.hits_bin, B.mbits, ws->status);
   } else {
     charges_kernel<false><<<pblocks, 256, 0, s>>>(n, n_live, A.pay, nullptr, nullptr, nullptr,
-                                                  sc, perm, cv, nullptr, nullptr, mbits,
+                                                  B.sc, B.perm, B.cv, nullptr, nullptr, B.mbits,
                                                   ws->status);
   }
   PRT_CHECK_CUDA(cudaGetLastError());
-  charge_scale_kernel<<<1, 1, 0, s>>>(mbits, kappa, sc);
-  PRT_CHECK_CUDA(cudaGetLastError());
-  charge_digits_kernel<<<pblocks, 256, 0, s>>>(n, cv, sc, cdig);
-  PRT_CHECK_CUDA(cudaGetLastError());
-  {
-    ScopedTimer timer(ws, PRT_TIME_DEPOSIT_GATHER, s);
-    if ((rc = launch_tc<false, false>(A, tiles, s))) return rc;
-  }
-  if ((rc = prt_dep_expand(mesh, vals, rho, j, s))) return rc;
-  if (stats) {
-    std::memset(stats, 0, sizeof(*stats));
-    if (norm && (rc = prt_dep_norm_stats(ws, n, scale_bin, hits_bin, stats, s))) return rc;
-    unsigned long long h[2] = {0, 0};
-    PRT_CHECK_CUDA(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, s));
-    PRT_CHECK_CUDA(cudaStreamSynchronize(s));
-    // candidates of the deposition pass (the normalisation pass adds the same)
-    stats->evaluated_pairs = (double)(h[0] / (norm ? 2 : 1)) * TM;
-  }
+  ws->tc_n = n;
   return PRT_OK;
+}
+
+// Step 3: charge digits from the maxima (device, [4] doubles), the
+// deposition pass into vals (sums == NULL) or into digit sums.
+int tc_deposit(const prt_mesh *mesh, prt_workspace *ws, prt_shape_function shape, long long n,
+               const BinGrid &G, TcPtrs &B, const double *maxima, double *sums, cudaStream_t s) {
+  TcArgs A;
+  tc_args(mesh, ws, shape, G, B, A);
+  A.sums = sums;
+  charge_scale_kernel<<<1, 1, 0, s>>>(reinterpret_cast<const unsigned long long *>(maxima),
+                                      tc_kappa(shape), B.sc);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  charge_digits_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, B.cv, B.sc, B.cdig);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  ScopedTimer timer(ws, PRT_TIME_DEPOSIT_GATHER, s);
+  return launch_tc<false, false>(A, ws->tc_tiles, s);
+}
+
+int tc_stats(prt_workspace *ws, bool norm, long long n, const TcPtrs &B,
+             prt_deposit_stats *stats, cudaStream_t s) {
+  int rc;
+  std::memset(stats, 0, sizeof(*stats));
+  if (norm && (rc = prt_dep_norm_stats(ws, n, B.scale_bin, B.hits_bin, stats, s))) return rc;
+  unsigned long long h[2] = {0, 0};
+  PRT_CHECK_CUDA(cudaMemcpyAsync(h, B.counters, sizeof(h), cudaMemcpyDeviceToHost, s));
+  PRT_CHECK_CUDA(cudaStreamSynchronize(s));
+  // candidates of the deposition pass (the normalisation pass adds the same)
+  stats->evaluated_pairs = (double)(h[0] / (norm ? 2 : 1)) * TM;
+  return PRT_OK;
+}
+
+}  // namespace
+
+int prt_deposit_shape_tc(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
+                         prt_shape_function shape, const double *iw, long long n,
+                         const double *x, const double *q, const double *v,
+                         const uint32_t *el, double *rho, double *j,
+                         prt_deposit_stats *stats, cudaStream_t s) {
+  TcPtrs B;
+  BinGrid G;
+  int rc;
+  if ((rc = tc_charges(mesh, ws, mode, shape, iw, n, x, q, v, el, stats != nullptr, s, B, G)))
+    return rc;
+  if ((rc = tc_deposit(mesh, ws, shape, n, G, B, reinterpret_cast<const double *>(B.mbits),
+                       nullptr, s)))
+    return rc;
+  if ((rc = prt_dep_expand(mesh, B.vals, rho, j, s))) return rc;
+  if (stats) return tc_stats(ws, mode == PRT_DEPOSIT_NORMALIZED, n, B, stats, s);
+  return PRT_OK;
+}
+
+// ------------------------------------------------------ C ABI: sharded form
+
+extern "C" int prt_mesh_position_count(const prt_mesh *mesh, int64_t *count) {
+  if (!mesh || !count) return PRT_ERR_INVALID_ARGUMENT;
+  *count = mesh->positions.count;
+  return PRT_OK;
+}
+
+extern "C" int prt_deposit_shape_charges(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
+                                         prt_shape_function shape, const double *iw, int64_t n,
+                                         const double *x, const double *q, const double *v,
+                                         const uint32_t *el, double *local_max,
+                                         prt_deposit_stats *stats, void *stream) {
+  if (!mesh || !ws || !local_max || n < 1 || n >= (1ll << 31)) return PRT_ERR_INVALID_ARGUMENT;
+  if (shape.alpha != 2 || !(shape.radius > 0)) return PRT_ERR_INVALID_ARGUMENT;
+  if (mode != PRT_DEPOSIT_PLAIN && mode != PRT_DEPOSIT_NORMALIZED) return PRT_ERR_INVALID_ARGUMENT;
+  if ((mode == PRT_DEPOSIT_NORMALIZED && !iw) || !x || !q) return PRT_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  TcPtrs B;
+  BinGrid G;
+  int rc;
+  if ((rc = tc_charges(mesh, ws, mode, shape, iw, n, x, q, v, el, stats != nullptr, s, B, G)))
+    return rc;
+  PRT_CHECK_CUDA(cudaMemcpyAsync(local_max, B.mbits, 4 * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, s));
+  if (stats) return tc_stats(ws, mode == PRT_DEPOSIT_NORMALIZED, n, B, stats, s);
+  return PRT_OK;
+}
+
+extern "C" int prt_deposit_shape_sums(const prt_mesh *mesh, prt_workspace *ws,
+                                      prt_shape_function shape, int64_t n,
+                                      const double *global_max, double *sums, void *stream) {
+  if (!mesh || !ws || !global_max || !sums || n < 1 || n != ws->tc_n)
+    return PRT_ERR_INVALID_ARGUMENT;
+  if (ws->tc_mesh_uid != mesh->uid || ws->tc_radius != shape.radius)
+    return PRT_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  TcPtrs B;
+  BinGrid G;
+  int rc;
+  if ((rc = tc_bins(mesh, shape, G))) return rc;
+  if ((rc = tc_buffers(mesh, ws, n, B))) return rc;
+  return tc_deposit(mesh, ws, shape, n, G, B, global_max, sums, s);
+}
+
+extern "C" int prt_deposit_shape_combine(const prt_mesh *mesh, prt_workspace *ws,
+                                         prt_shape_function shape, const double *global_max,
+                                         const double *sums, double *rho, double *j,
+                                         void *stream) {
+  if (!mesh || !ws || !global_max || !sums || !(shape.radius > 0))
+    return PRT_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  const PositionSet &PS = mesh->positions;
+  int rc;
+  char *misc = (char *)ws_buffer(ws, PRT_WS_TC_MISC, 1024 + 16 * (size_t)ws->tc_tiles, &rc);
+  if (!misc) return rc;
+  TcScales *sc = (TcScales *)(misc + 256);
+  double *vals = (double *)ws_buffer(ws, PRT_WS_DEP_VALUES, 4 * sizeof(double) * PS.count, &rc);
+  if (!vals) return rc;
+  charge_scale_kernel<<<1, 1, 0, s>>>(reinterpret_cast<const unsigned long long *>(global_max),
+                                      tc_kappa(shape), sc);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  combine_kernel<<<prt_grid_blocks(PS.count, 256), 256, 0, s>>>(PS.count, sums, sc, vals);
+  PRT_CHECK_CUDA(cudaGetLastError());
+  return prt_dep_expand(mesh, vals, rho, j, s);
 }

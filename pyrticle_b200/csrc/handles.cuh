@@ -28,6 +28,7 @@ enum {
   PRT_WS_TC_WDIG,     // tensor-core deposition: position weight digits
   PRT_WS_TC_PART,     // tensor-core deposition: per-particle sums, values and digits
   PRT_WS_TC_MISC,     // tensor-core deposition: scales, counters, tile order
+  PRT_WS_TC_TILESET,  // tensor-core deposition: tile starts and boxes (per radius)
   PRT_WS_SLOTS
 };
 
@@ -61,12 +62,6 @@ struct PositionSet {
     const double *spheres = nullptr;    // [groups][4], bin order
     const uint32_t *ranges = nullptr;   // [groups][2]: first position, count
   } centre_bins;
-  // tiles of the tensor-core deposition: runs of <= 128 consecutive
-  // positions that never straddle a Morton cell of about PRT_TILE_TARGET
-  // positions, with their bounding boxes
-  long long tiles = 0;
-  const uint32_t *tile_starts = nullptr;  // [tiles + 1]
-  const double *tile_boxes = nullptr;     // [tiles][6]: centre xyz, half extent xyz
 };
 
 struct prt_mesh {
@@ -76,6 +71,12 @@ struct prt_mesh {
   double box_lo[3], box_hi[3];             // node bounding box of the mesh
   PositionSet positions;
   unsigned long long uid = 0;              // unique per created mesh (workspace caches)
+  // host copies of the positions [count][3] and their Morton keys (21 bits
+  // per axis over the cube of side morton_ext at box_lo): the tensor-core
+  // deposition cuts its tiles from them per shape radius
+  std::vector<double> pos_host;
+  std::vector<uint64_t> pos_key;
+  double morton_ext = 1;
 };
 
 // CUDA-event timing of the main kernels (prt_workspace_timing).
@@ -95,6 +96,8 @@ struct prt_workspace {
   // this shape radius
   unsigned long long tc_mesh_uid = 0;
   double tc_radius = 0;
+  long long tc_tiles = 0;   // tiles of that mesh and radius (PRT_WS_TC_TILESET)
+  long long tc_n = -1;      // particles of the last tensor-core charges step
   DevStatus *status = nullptr;
   bool timing = false;
   KernelTimer timers[PRT_TIME_CATEGORIES];
@@ -138,7 +141,8 @@ constexpr double PRT_GROUP_TARGET = 24.0;
 #define PRT_WIDE_CELL_BITS 1
 #endif
 
-// target positions per Morton cell when cutting the tensor-core tiles
+// target positions per Morton cell when cutting the tensor-core tiles (the
+// cells are also at most two shape radii wide)
 #ifndef PRT_TILE_TARGET
 #define PRT_TILE_TARGET 128.0
 #endif

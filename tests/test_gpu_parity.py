@@ -350,8 +350,8 @@ def test_grid_deposit_and_remap(setup, weights):
 
 
 def test_mixed_precision_deposit_error_bounds():
-    """The chosen form: FP32 shape weights and batch sums, FP64 combine.
-    rho and j within 1e-5 relative L2 of the FP64 form (config2's bound), on a
+    """The chosen form (tensor-core deposition): rho and j within 1e-5
+    relative L2 of the FP64 form (config2's bound), on a
     config2-like case (order 3, radius 0.08 cm) at reduced size."""
     w = problems.make("config2", scale=0.005, cubes=(16, 16, 64))
     m = make_method(w)
@@ -373,5 +373,6 @@ def test_mixed_precision_normalized_charge():
     rho, _ = m.deposit_densities(s)
     iw = m.depositor.integral_weights
     total = float((rho.reshape(-1, len(iw)) @ iw * w.mesh.jacobians).sum())
-    # FP32 batch sums: the deposited charge is exact to FP32 rounding
-    assert total == pytest.approx(float(w.charges.sum()), rel=1e-6)
+    # integer weights summed exactly against the same integer weights'
+    # integrals: the deposited charge is exact to FP64 rounding
+    assert total == pytest.approx(float(w.charges.sum()), rel=1e-14)

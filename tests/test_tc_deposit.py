@@ -192,3 +192,54 @@ def test_tc_and_simt_forms_agree(small_workload):
     r2, j2 = m.depositor.deposit_densities_device(s, precision="mixed_simt")
     assert rel_l2(r1.cpu().numpy(), r2.cpu().numpy()) < 2 * MIXED_TOL
     assert rel_l2(j1.cpu().numpy(), j2.cpu().numpy()) < 2 * MIXED_TOL
+
+
+@pytest.mark.parametrize("normalized", [False, True])
+def test_tc_sharded_sums_are_bitwise_independent_of_the_split(small_workload, normalized):
+    """Two ranks emulated on one GPU (two methods, each with its own
+    workspace, the particles split in two): the charge maxima combined with
+    max, the digit sums added, then combined, give bitwise the same rho and
+    j as all particles on one GPU, by the single call and by the protocol."""
+    from pyrticle_b200.sharding import deposit_densities_exact
+    w = small_workload
+    Dep = NormalizedShapeFunctionDepositor if normalized else ShapeFunctionDepositor
+    ms = [method(w.mesh, w.order, w.shape_radius, Dep("mixed"), w.nodes) for _ in range(3)]
+    full = state(ms[0], w.positions, w.momenta, w.charges, w.masses)
+    rho1, j1 = ms[0].depositor.deposit_densities_device(full, precision="mixed")
+    rho2, j2 = deposit_densities_exact(ms[0], full)
+    assert torch.equal(rho1, rho2) and torch.equal(j1, j2)
+    n = len(w.positions)
+    cut = n // 3
+    parts = [state(ms[1], w.positions[:cut], w.momenta[:cut], w.charges[:cut], w.masses[:cut]),
+             state(ms[2], w.positions[cut:], w.momenta[cut:], w.charges[cut:], w.masses[cut:])]
+    from pyrticle_b200 import _lib
+    import ctypes as C
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    sf = ms[0].depositor.shape_function
+    desc = _lib.ShapeFunctionDesc(sf.radius, sf.exponent, sf.normalizer)
+    iw = getattr(ms[0].depositor, "integral_weights", None)
+    npos = C.c_int64()
+    _lib.check(ms[0].lib.prt_mesh_position_count(ms[0].mesh_data.handle, C.byref(npos)))
+    maxima = []
+    for m, s in zip(ms[1:], parts):
+        mx = torch.zeros(4, dtype=torch.float64, device="cuda")
+        v = m.velocities_device(s)
+        _lib.check(m.lib.prt_deposit_shape_charges(
+            m.mesh_data.handle, m.workspace, m.depositor.mode, desc,
+            _lib.ptr(iw) if iw is not None else None, len(s), s.x.data_ptr(), s.q.data_ptr(),
+            v.data_ptr(), s.el.data_ptr(), mx.data_ptr(), None, stream))
+        maxima.append(mx)
+    gmax = torch.maximum(maxima[0], maxima[1])
+    total = torch.zeros((16, npos.value), dtype=torch.float64, device="cuda")
+    for m, s in zip(ms[1:], parts):
+        part = torch.zeros_like(total)
+        _lib.check(m.lib.prt_deposit_shape_sums(m.mesh_data.handle, m.workspace, desc, len(s),
+                                                gmax.data_ptr(), part.data_ptr(), stream))
+        total += part
+    rho3 = torch.empty_like(rho1)
+    j3 = torch.empty_like(j1)
+    _lib.check(ms[0].lib.prt_deposit_shape_combine(
+        ms[0].mesh_data.handle, ms[0].workspace, desc, gmax.data_ptr(), total.data_ptr(),
+        rho3.data_ptr(), j3.data_ptr(), stream))
+    ms[0].check_status()
+    assert torch.equal(rho1, rho3) and torch.equal(j1, j3)
