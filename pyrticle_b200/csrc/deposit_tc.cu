@@ -82,7 +82,6 @@ constexpr uint32_t TMEM_COLS = 256;
 constexpr uint32_t COL_ACC = 128;  // accumulators: weight digit d at +16 d, indicator at +48
 constexpr int FDIG = 3;            // weight digits (bytes 2, 1, 0 of the weight)
 constexpr float SIGMA = 1448.0f;   // 4 SIGMA^2 < 2^23
-constexpr unsigned SPIN = 1u << 22;  // try_wait rounds before a wait gives up
 constexpr int FLUSH_CHUNKS = 256;    // int32 accumulation window (256 * 128 * 255 * 128 < 2^31)
 constexpr int CDIG = 6, JDIG = 3, WDIG = 6;
 
@@ -98,6 +97,7 @@ struct Smem {
   uint32_t seg_start[MAXSEG];    // first bin-order particle of a segment
   uint32_t seg_pref[MAXSEG + 1]; // stream offset of a segment
   uint8_t seg_img[MAXSEG];       // periodic image (qx+1) + 3 (qy+1) + 9 (qz+1)
+  uint32_t seg_row[MAXSEG];      // bin row of a segment: wy | wz << 16
   unsigned long long bar_s, bar_a;
   uint32_t tmem;
   int tail, cursor, nseg, total, abort;
@@ -114,6 +114,9 @@ struct TcArgs {
   const uint4 *__restrict__ tile_ops;   // [tiles][256] position operands
   const uint4 *__restrict__ wdig;       // [tiles][128] weight digits
   const uint4 *__restrict__ cdig;       // [n] charge digits, bin order
+  // [n] bin order: position relative to the particle's bin origin (FP32)
+  // and the bin's x index (int bits)
+  const float4 *__restrict__ cpos;
   const uint32_t *__restrict__ order;   // launch order of the tiles (or NULL)
   double radius, inv_radius;
   unsigned long long *__restrict__ norm_hi, *__restrict__ norm_lo;  // [n], bin order
@@ -163,15 +166,20 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
       : "memory");
 }
 
+// Bounded wait for the phase of `parity`. Each try_wait may suspend the
+// thread until the phase completes, for at most WAIT_NS, so waiting warps
+// take no issue slots; false after WAIT_TRIES tries (about one second).
+constexpr unsigned WAIT_NS = 1000000;
+constexpr unsigned WAIT_TRIES = 1024;
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (unsigned k = 0; k < SPIN; ++k) {
+  for (unsigned k = 0; k < WAIT_TRIES; ++k) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
         "selp.b32 %0, 1, 0, P1;\n\t}\n"
         : "=r"(ok)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "r"(WAIT_NS)
         : "memory");
     if (ok) return true;
   }
@@ -199,17 +207,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&r)[32]) {
         "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
         "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
         "=r"(r[31])
-      : "r"(addr)
-      : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(addr)
       : "memory");
 }
@@ -295,7 +292,7 @@ __device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], cons
   bool overflow = false;
   for (int r0 = 0; r0 < nrows; r0 += 32) {
     const int r = r0 + lane;
-    uint32_t s_start[3], s_len[3];
+    uint32_t s_start[3], s_len[3], s_row = 0;
     uint8_t s_img[3];
     int cnt = 0;
     uint32_t len = 0;
@@ -323,6 +320,7 @@ __device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], cons
         bx0 = max(bx0, ulo[0]);
         bx1 = min(bx1, uhi[0]);
         const long long row = (long long)G.dims[0] * (wy + (long long)G.dims[1] * wz);
+        s_row = (uint32_t)wy | ((uint32_t)wz << 16);
         int bx = bx0;
         while (bx <= bx1) {
           int wx = bx, qx = 0, seg_end = bx1;
@@ -367,6 +365,7 @@ __device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], cons
         S.seg_start[sbase + i] = s_start[i];
         S.seg_pref[sbase + i] = lbase;
         S.seg_img[sbase + i] = s_img[i];
+        S.seg_row[sbase + i] = s_row;
       }
       lbase += s_len[i];
     }
@@ -385,45 +384,83 @@ __device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], cons
   }
 }
 
-// Stages candidates into the ring until it holds `target` slots or the
-// stream ends (every warp; at most 32 slots per warp past the target).
+// A warp's place in its tile's candidate stream: the warp stages the
+// segments warp, warp + 8, ... of the tile, 32 particles (a batch) at a time,
+// with three batches loaded ahead, each in its own registers (a batch's
+// values are read only when it is processed, then the set is refilled).
+struct Batch {
+  int seg, off;  // seg < 0: none
+  float4 pos;    // the lane's particle: offset from its bin origin, bin x index
+  uint4 dig;     // its charge digits (deposition pass)
+};
+
+struct Cursor {
+  int cseg, coff;  // the next batch to load
+  int rot;         // the set that holds the oldest loaded batch
+  Batch q0, q1, q2;
+};
+
+template <bool NORM>
+__device__ __forceinline__ void next_batch(const Smem &S, const TcArgs &A, Cursor &C, Batch &B,
+                                           int lane) {
+  B.seg = C.cseg < S.nseg ? C.cseg : -1;
+  B.off = C.coff;
+  if (B.seg < 0) return;
+  const int len = (int)(S.seg_pref[B.seg + 1] - S.seg_pref[B.seg]);
+  if (B.off + lane < len) {
+    const size_t k = (size_t)S.seg_start[B.seg] + B.off + lane;
+    B.pos = A.cpos[k];
+    if (!NORM) B.dig = A.cdig[k];
+  }
+  C.coff += 32;
+  if (C.coff >= len) {
+    C.coff = 0;
+    C.cseg += THREADS / 32;
+  }
+}
+
+template <bool NORM>
+__device__ __forceinline__ void cursor_init(const Smem &S, const TcArgs &A, Cursor &C, int warp,
+                                            int lane) {
+  C.cseg = warp;
+  C.coff = 0;
+  C.rot = 0;
+  C.q0.pos = C.q1.pos = C.q2.pos = make_float4(0, 0, 0, 0);
+  C.q0.dig = C.q1.dig = C.q2.dig = make_uint4(0, 0, 0, 0);
+  next_batch<NORM>(S, A, C, C.q0, lane);
+  next_batch<NORM>(S, A, C, C.q1, lane);
+  next_batch<NORM>(S, A, C, C.q2, lane);
+}
+
+// Stages candidates into the ring until it holds `target` slots or every
+// warp's segments are exhausted (every warp; at most 32 slots per warp past
+// the target).
 template <bool NORM>
 __device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const double c[3],
-                                     const float hf[3], int target, int lane) {
+                                     const float hf[3], int target, int lane, Cursor &C) {
   const BinGrid &G = A.G;
   const float rcf = (float)(A.radius * (1 + 1e-5));
   const float rc4 = 4.0f * rcf * rcf;
   const float inv_a = (float)A.inv_radius;
-  const int total = S.total, nseg = S.nseg;
-  for (;;) {
-    const int tail = __shfl_sync(0xffffffffu, *(volatile int *)&S.tail, 0);
-    if (tail >= target) break;
-    int t0 = 0;
-    if (lane == 0) t0 = atomicAdd(&S.cursor, 32);
-    t0 = __shfl_sync(0xffffffffu, t0, 0);
-    if (t0 >= total) break;
-    const int idx = t0 + lane;
+  // culls batch B into the ring, then refills B with the warp's next batch
+  auto process = [&](Batch &B) {
+    const int len = (int)(S.seg_pref[B.seg + 1] - S.seg_pref[B.seg]);
+    const bool valid = B.off + lane < len;
+    const uint32_t k = S.seg_start[B.seg] + (uint32_t)(B.off + lane);
+    const int img = S.seg_img[B.seg];
+    const uint32_t brow = S.seg_row[B.seg];
+    // bin origins relative to the tile centre (FP64), periodic image included
+    const double ox = G.origin[0] + (img % 3 - 1) * G.period[0] - c[0];
+    const float oy = (float)(G.origin[1] + (double)(brow & 0xffffu) * G.w[1] +
+                             ((img / 3) % 3 - 1) * G.period[1] - c[1]);
+    const float oz = (float)(G.origin[2] + (double)(brow >> 16) * G.w[2] +
+                             (img / 9 - 1) * G.period[2] - c[2]);
     bool in = false;
     float w0 = 0, w1 = 0, w2 = 0;
-    uint32_t k = 0;
-    if (idx < total) {
-      int lo = 0, hi = nseg - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if ((int)S.seg_pref[mid] <= idx)
-          lo = mid;
-        else
-          hi = mid - 1;
-      }
-      k = S.seg_start[lo] + (uint32_t)(idx - (int)S.seg_pref[lo]);
-      const int img = S.seg_img[lo];
-      const double sx = (img % 3 - 1) * G.period[0] - c[0];
-      const double sy = ((img / 3) % 3 - 1) * G.period[1] - c[1];
-      const double sz = (img / 9 - 1) * G.period[2] - c[2];
-      const double2 xy = A.pay[4 * (size_t)k], zq = A.pay[4 * (size_t)k + 1];
-      w0 = (float)(xy.x + sx);
-      w1 = (float)(xy.y + sy);
-      w2 = (float)(zq.x + sz);
+    if (valid) {
+      w0 = (float)fma((double)__float_as_int(B.pos.w), G.w[0], ox) + B.pos.x;
+      w1 = oy + B.pos.y;
+      w2 = oz + B.pos.z;
       // rounded-box cull: per axis 2 max(|w| - half, 0) = d + |d|
       const float d0 = fabsf(w0) - hf[0], d1 = fabsf(w1) - hf[1], d2 = fabsf(w2) - hf[2];
       const float e0 = d0 + fabsf(d0), e1 = d1 + fabsf(d1), e2 = d2 + fabsf(d2);
@@ -442,8 +479,21 @@ __device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const double c[3]
       if (NORM)
         S.slot_id[slot] = k;
       else
-        *reinterpret_cast<uint4 *>(S.bdig + (size_t)slot * 16) = A.cdig[k];
+        *reinterpret_cast<uint4 *>(S.bdig + (size_t)slot * 16) = B.dig;
     }
+    next_batch<NORM>(S, A, C, B, lane);
+  };
+  for (;;) {
+    const int tail = __shfl_sync(0xffffffffu, *(volatile int *)&S.tail, 0);
+    const int bseg = C.rot == 0 ? C.q0.seg : C.rot == 1 ? C.q1.seg : C.q2.seg;
+    if (tail >= target || bseg < 0) break;
+    if (C.rot == 0)
+      process(C.q0);
+    else if (C.rot == 1)
+      process(C.q1);
+    else
+      process(C.q2);
+    C.rot = C.rot == 2 ? 0 : C.rot + 1;
   }
 }
 
@@ -591,6 +641,8 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
 
   bool ok = S.abort == 0;
   int issued_s = 0, issued_a = 0, waited_s = 0, waited_a = 0;
+  Cursor cur;
+  cursor_init<NORM>(S, A, cur, warp, lane);
   int valid = 0;
 
   // readout of a normalisation chunk: per candidate its sum over the tile
@@ -650,7 +702,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   int window = 0;       // chunks in the current int32 deposition window
   int valid_prev = 0;   // valid slots of the chunk whose accumulation is in flight
   if (ok) {
-    fill<NORM>(S, A, c, hf, NC, lane);
+    fill<NORM>(S, A, c, hf, NC, lane, cur);
     __syncthreads();
     valid = min(S.tail, NC);
     if (valid > 0 && valid < NC) pad_chunk(S, valid, NC, tid);
@@ -680,7 +732,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     }
     __syncthreads();
     // (2) stage chunk k+1 while the tensor cores score chunk k
-    fill<NORM>(S, A, c, hf, (k + 2) * NC, lane);
+    fill<NORM>(S, A, c, hf, (k + 2) * NC, lane, cur);
     __syncthreads();
     const int valid_next = min(max(S.tail - (k + 1) * NC, 0), NC);
     if (valid_next > 0 && valid_next < NC)
@@ -789,6 +841,27 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
 }
 
 // ------------------------------------------------------------ preparation
+
+// The candidates' compact positions (bin order): the offset from the
+// particle's bin origin in FP32 (below a bin width: exact to ~1e-7 of it) and
+// the bin's x index.
+__global__ void candidate_positions_kernel(long long n, const uint32_t *__restrict__ perm,
+                                           const double *__restrict__ x, BinGrid G,
+                                           float4 *__restrict__ out) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t i = perm[s];
+  float d[3];
+  int b0 = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double xa = x[a * n + i];
+    const int b = bin_coord(G, a, xa);
+    d[a] = (float)(xa - (G.origin[a] + b * G.w[a]));
+    if (a == 0) b0 = b;
+  }
+  out[s] = make_float4(d[0], d[1], d[2], __int_as_float(b0));
+}
 
 // Position operands of every tile, K-major: row u of tile t at
 // [t][K chunk][u][16 B] (rows past the tile's positions are zero).
@@ -985,32 +1058,6 @@ __global__ void charge_digits_kernel(long long n, const double *__restrict__ cv,
   out[k] = pack16(b);
 }
 
-// Work estimate per tile: the particles in the bin rows of its box grown by
-// the radius (periodic images ignored), keyed for a descending sort so that
-// the heaviest tiles start first and the light ones fill the tail of the
-// launch. Each tile is one CTA whatever the order, so no result changes.
-__global__ void tile_work_kernel(long long tiles, const double *__restrict__ tile_boxes,
-                                 BinGrid G, const uint32_t *__restrict__ starts, double radius,
-                                 uint32_t *__restrict__ work, uint32_t *__restrict__ ids) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= tiles) return;
-  int lo[3], hi[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const double c = tile_boxes[6 * t + d], h = tile_boxes[6 * t + 3 + d] + radius;
-    lo[d] = max(0, min(G.dims[d] - 1, bin_floor(G, d, c - h)));
-    hi[d] = max(0, min(G.dims[d] - 1, bin_floor(G, d, c + h)));
-  }
-  unsigned long long wsum = 0;
-  for (int bz = lo[2]; bz <= hi[2]; ++bz)
-    for (int by = lo[1]; by <= hi[1]; ++by) {
-      const long long row = (long long)G.dims[0] * (by + (long long)G.dims[1] * bz);
-      wsum += starts[row + hi[0] + 1] - starts[row + lo[0]];
-    }
-  work[t] = (uint32_t)min(wsum, 0xffffffffull);
-  ids[t] = (uint32_t)t;
-}
-
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // rho, j of every position from summed digit sums (sharded form, step 3)
@@ -1043,10 +1090,10 @@ struct TcPtrs {
   uint32_t *hits;
   double *cv;
   uint4 *cdig;
+  float4 *cpos;
   double *scale_bin, *hits_bin;
   unsigned long long *mbits, *counters;
   TcScales *sc;
-  uint32_t *order_buf;
   uint4 *tile_ops;
   const uint32_t *tile_starts;
   const double *tile_boxes;
@@ -1125,7 +1172,7 @@ int tc_buffers(const prt_mesh *mesh, prt_workspace *ws, long long n, TcPtrs &B) 
   const size_t b_cv = align256(32 * (size_t)n), b_dig = align256(16 * (size_t)n);
   const size_t b_f64 = align256(8 * (size_t)n);
   char *part = (char *)ws_buffer(ws, PRT_WS_TC_PART,
-                                 2 * b_u64 + b_u32 + b_cv + b_dig + 2 * b_f64, &rc);
+                                 2 * b_u64 + b_u32 + b_cv + 2 * b_dig + 2 * b_f64, &rc);
   if (!part) return rc;
   B.nhi = (unsigned long long *)part;
   B.nlo = (unsigned long long *)(part + b_u64);
@@ -1134,14 +1181,13 @@ int tc_buffers(const prt_mesh *mesh, prt_workspace *ws, long long n, TcPtrs &B) 
   B.cdig = (uint4 *)(part + 2 * b_u64 + b_u32 + b_cv);
   B.scale_bin = (double *)(part + 2 * b_u64 + b_u32 + b_cv + b_dig);
   B.hits_bin = (double *)(part + 2 * b_u64 + b_u32 + b_cv + b_dig + b_f64);
-  // small: maxima of |c|, |c v|, W (bits), the candidate counter, the
-  // scales; then the tiles' launch order (heaviest first)
-  char *misc = (char *)ws_buffer(ws, PRT_WS_TC_MISC, 1024 + 16 * (size_t)tiles, &rc);
+  B.cpos = (float4 *)(part + 2 * b_u64 + b_u32 + b_cv + b_dig + 2 * b_f64);
+  // small: maxima of |c|, |c v|, W (bits), the candidate counter, the scales
+  char *misc = (char *)ws_buffer(ws, PRT_WS_TC_MISC, 1024, &rc);
   if (!misc) return rc;
   B.mbits = (unsigned long long *)misc;  // [8]
   B.counters = B.mbits + 8;             // [4]
   B.sc = (TcScales *)(misc + 256);
-  B.order_buf = (uint32_t *)(misc + 1024);
   B.tile_ops = (uint4 *)ws_buffer(ws, PRT_WS_TC_TILES, 4096 * (size_t)tiles, &rc);
   if (!B.tile_ops) return rc;
   const size_t b_ts = align256(4 * (size_t)(tiles + 1));
@@ -1180,7 +1226,8 @@ void tc_args(const prt_mesh *mesh, prt_workspace *ws, prt_shape_function shape,
   A.tile_ops = B.tile_ops;
   A.wdig = nullptr;
   A.cdig = B.cdig;
-  A.order = ws->tc_tiles > 1 ? B.order_buf + 3 * ws->tc_tiles : nullptr;
+  A.cpos = B.cpos;
+  A.order = nullptr;  // Morton order: CTAs running together share candidates in L2
   A.radius = shape.radius;
   A.inv_radius = 1.0 / shape.radius;
   A.norm_hi = B.nhi;
@@ -1216,21 +1263,9 @@ int tc_charges(const prt_mesh *mesh, prt_workspace *ws, int32_t mode, prt_shape_
   }
   // buffers may have moved while staging grew the workspace
   if ((rc = tc_buffers(mesh, ws, n, B))) return rc;
+  candidate_positions_kernel<<<prt_grid_blocks(n, 256), 256, 0, s>>>(n, B.perm, x, G, B.cpos);
+  PRT_CHECK_CUDA(cudaGetLastError());
   PRT_CHECK_CUDA(cudaMemsetAsync(B.mbits, 0, 256, s));
-  if (tiles > 1) {
-    uint32_t *wk = B.order_buf, *ids = wk + tiles, *wk_out = wk + 2 * tiles,
-             *ids_out = wk + 3 * tiles;
-    tile_work_kernel<<<prt_grid_blocks(tiles, 256), 256, 0, s>>>(tiles, B.tile_boxes, G,
-                                                                 P.starts, shape.radius, wk, ids);
-    PRT_CHECK_CUDA(cudaGetLastError());
-    size_t tb = 0;
-    PRT_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, wk, wk_out, ids,
-                                                             ids_out, (int)tiles, 0, 32, s));
-    void *tmp = ws_buffer(ws, PRT_WS_CUB, tb, &rc);
-    if (!tmp) return rc;
-    PRT_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tb, wk, wk_out, ids, ids_out,
-                                                             (int)tiles, 0, 32, s));
-  }
   TcArgs A;
   tc_args(mesh, ws, shape, G, B, A);
   const unsigned pblocks = (unsigned)((n + 255) / 256);
@@ -1374,7 +1409,7 @@ extern "C" int prt_deposit_shape_combine(const prt_mesh *mesh, prt_workspace *ws
   cudaStream_t s = (cudaStream_t)stream;
   const PositionSet &PS = mesh->positions;
   int rc;
-  char *misc = (char *)ws_buffer(ws, PRT_WS_TC_MISC, 1024 + 16 * (size_t)ws->tc_tiles, &rc);
+  char *misc = (char *)ws_buffer(ws, PRT_WS_TC_MISC, 1024, &rc);
   if (!misc) return rc;
   TcScales *sc = (TcScales *)(misc + 256);
   double *vals = (double *)ws_buffer(ws, PRT_WS_DEP_VALUES, 4 * sizeof(double) * PS.count, &rc);
