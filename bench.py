@@ -466,9 +466,13 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     from pyrticle_b200 import _lib, problems
-    from pyrticle_b200.sharding import allreduce_densities, max_over_ranks
+    from pyrticle_b200.sharding import (allreduce_densities, deposit_densities_exact,
+                                        max_over_ranks)
 
-    w = problems.make(args.workload, scale=args.scale, seed=1 + rank)
+    # weak scaling: every rank holds the particles of its slab of a beam
+    # world times larger (its contiguous block of the element-sorted order)
+    w = problems.make(args.workload, scale=args.scale, seed=1 + rank,
+                      zslab=(rank, world) if world > 1 and args.workload != "config4" else None)
     m, sf = build_method(w, torch, normalized=args.depositor == "normalized")
     s = m.make_state()
     m.add_particles_from_arrays(s, w.positions, w.momenta, w.charges, w.masses)
@@ -479,9 +483,16 @@ def main():
     prec = {"fp64": 0, "mixed": 1}
 
     def one_step(form):
-        """One step of the given form: 5 fused RK stages + the deposition."""
+        """One step of the given form: 5 fused RK stages + the deposition.
+        With several ranks the chosen form deposits through the exact sharded
+        protocol (charge maxima all-reduced, integer digit sums all-reduced:
+        bitwise the same for any rank count); the FP64 form all-reduces rho
+        and j."""
         m.depositor.precision = form
         try:
+            if world > 1 and form == "mixed":
+                m.step(s, fields, w.dt, steps=1, deposit=False, check=False, precision=prec[form])
+                return deposit_densities_exact(m, s)
             rho, j = m.step(s, fields, w.dt, steps=1, check=False, precision=prec[form])
         finally:
             m.depositor.precision = "fp64"
@@ -574,11 +585,12 @@ def main():
         def one_step_on(st):
             m.depositor.precision = "mixed"
             try:
+                if world > 1:
+                    m.step(st, fields, w.dt, steps=1, deposit=False, check=False, precision=1)
+                    return deposit_densities_exact(m, st)
                 rho, j = m.step(st, fields, w.dt, steps=1, check=False, precision=1)
             finally:
                 m.depositor.precision = "fp64"
-            if world > 1:
-                allreduce_densities(rho, j)
             return rho, j
 
         if world > 1:
@@ -699,8 +711,9 @@ def main():
                        "nodes": nn, "order": w.order, "form": "mixed",
                        "depositor": args.depositor,
                        "l2": f"inputs larger than L2 ({216 * n / 1e9:.1f} GB particle state per stage)",
-                       "parallelism": f"particles sharded over {world} GPU(s), NCCL "
-                                      "all-reduce of rho/j" if world > 1 else "1 GPU"},
+                       "parallelism": f"particles sharded over {world} GPU(s) (z slabs of "
+                                      "the beam), NCCL all-reduce of the integer digit sums "
+                                      "per node position" if world > 1 else "1 GPU"},
             "clocks": clk, "gpu_launches": None, "roofline": roofline,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kernel.items()},
             "pairs_per_deposition": {"positions": pairs, "nodes": node_pairs,

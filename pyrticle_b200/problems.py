@@ -140,8 +140,16 @@ def stable_dt(mesh, courant=0.3):
     return courant * float(mesh.inradii().min()) / U.VACUUM_LIGHT_SPEED()
 
 
-def make(name: str, scale: float = 1.0, cubes=None, steps=None, seed=1) -> Workload:
-    """Build a named workload; ``scale`` multiplies the particle count."""
+def make(name: str, scale: float = 1.0, cubes=None, steps=None, seed=1,
+         zslab=None) -> Workload:
+    """Build a named workload; ``scale`` multiplies the particle count.
+
+    ``zslab=(rank, world)`` (beam workloads): the rank's share of a beam of
+    ``world`` times the particles, i.e. the particles of the world-times-larger
+    beam whose z falls in the rank's slab of the beam's z range (the beam is
+    uniform in z, so each slab holds the same count). Elements are numbered
+    with z slowest, so this is the rank's contiguous block of the
+    element-sorted global particle order."""
     lo = np.zeros(3)
     hi = np.array([1 * CM, 1 * CM, 4 * CM])
     axis_xy = (0.5 * CM, 0.5 * CM)
@@ -170,7 +178,11 @@ def make(name: str, scale: float = 1.0, cubes=None, steps=None, seed=1) -> Workl
         x, p = _bunch(n, rng, 0.1 * CM, 0.05 * CM, (0.5 * CM, 0.5 * CM, 2 * CM), 5.0,
                       lo, hi)
     else:
-        x, p = _beam(n, rng, 0.25 * CM, 0.5 * CM, 3.5 * CM, 2.0, axis_xy)
+        zlo, zhi = 0.5 * CM, 3.5 * CM
+        if zslab is not None:
+            r, nr = zslab
+            zlo, zhi = zlo + (zhi - zlo) * r / nr, zlo + (zhi - zlo) * (r + 1) / nr
+        x, p = _beam(n, rng, 0.25 * CM, zlo, zhi, 2.0, axis_xy)
     basis = theta = None
     if name in ("config0", "config3"):
         basis = focusing_basis(nodes, axis_xy)
