@@ -912,9 +912,6 @@ int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
   P.count = npos;
   // host copies for the tensor-core tiles, which are cut per shape radius
   m->pos_host = pos;
-  m->pos_key.resize(npos);
-  for (long long u = 0; u < npos; ++u) m->pos_key[u] = key[order[run_starts[u]]];
-  m->morton_ext = ext;
   int rc;
   if ((rc = upload_vec(pos, &P.pos))) return rc;
   if ((rc = upload_vec(node_to_pos, &P.node_to_pos))) return rc;

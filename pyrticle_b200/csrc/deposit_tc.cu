@@ -7,9 +7,9 @@
 // (dep_normshape.hpp:125-199). Both are sums over (particle, node position)
 // pairs within the radius a of S(r) = N (a - r^2/a)^2 = N a^2 (1 - r^2/a^2)^2.
 //
-// Here the distinct node positions are cut into tiles of <= 128 (Morton
-// runs within cells at most two radii wide, cut per shape radius) and each
-// CTA takes one tile:
+// Here the distinct node positions are cut into tiles of <= 128 (compact
+// boxes at most two radii wide from recursive bisection, cut per shape
+// radius; all but a few tiles hold exactly 128) and each CTA takes one tile:
 //
 //  1. candidates: the particles of the bin rows within the radius of the
 //     tile's box (particles binned and packed in bin order, binning.cuh),
@@ -109,7 +109,8 @@ struct TcArgs {
   BinGrid G;
   const double2 *__restrict__ pay;      // [n][4] bin-order payload (x, y | z, q | ...)
   const uint32_t *__restrict__ starts;  // [nbins + 1]
-  const uint32_t *__restrict__ tile_starts;
+  const uint32_t *__restrict__ tile_starts;  // [tiles + 1] into tile_rows
+  const uint32_t *__restrict__ tile_rows;    // position of each tile row
   const double *__restrict__ tile_boxes; // [tiles][6]: centre xyz, half extent xyz
   const uint4 *__restrict__ tile_ops;   // [tiles][256] position operands
   const uint4 *__restrict__ wdig;       // [tiles][128] weight digits
@@ -817,7 +818,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
         double T[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) T[i] = tsum[row][i];
-        const long long u = p0 + row;
+        const long long u = A.tile_rows[p0 + row];
         if (A.sums) {
 #pragma unroll
           for (int i = 0; i < 16; ++i) A.sums[i * A.npos + u] = T[i];
@@ -866,6 +867,7 @@ __global__ void candidate_positions_kernel(long long n, const uint32_t *__restri
 // Position operands of every tile, K-major: row u of tile t at
 // [t][K chunk][u][16 B] (rows past the tile's positions are zero).
 __global__ void tile_operands_kernel(long long tiles, const uint32_t *__restrict__ tile_starts,
+                                     const uint32_t *__restrict__ tile_rows,
                                      const double *__restrict__ tile_boxes,
                                      const double *__restrict__ pos, double inv_radius,
                                      uint4 *__restrict__ out) {
@@ -876,7 +878,7 @@ __global__ void tile_operands_kernel(long long tiles, const uint32_t *__restrict
   const int npt = (int)(tile_starts[t + 1] - p0);
   uint4 k0 = make_uint4(0, 0, 0, 0), k1 = make_uint4(0, 0, 0, 0);
   if (u < npt) {
-    const long long p = p0 + u;
+    const long long p = tile_rows[p0 + u];
     const double ux = (pos[3 * p] - tile_boxes[6 * t]) * inv_radius;
     const double uy = (pos[3 * p + 1] - tile_boxes[6 * t + 1]) * inv_radius;
     const double uz = (pos[3 * p + 2] - tile_boxes[6 * t + 2]) * inv_radius;
@@ -970,6 +972,7 @@ __device__ __forceinline__ uint4 pack16(const uint8_t b[16]) {
 // base-256 digits (columns 0-5), a one in column 6 (the indicator sum), per
 // tile row.
 __global__ void weight_digits_kernel(long long tiles, const uint32_t *__restrict__ tile_starts,
+                                     const uint32_t *__restrict__ tile_rows,
                                      const double *__restrict__ W, const TcScales *sc,
                                      uint4 *__restrict__ out) {
   const long long t = blockIdx.x;
@@ -981,7 +984,7 @@ __global__ void weight_digits_kernel(long long tiles, const uint32_t *__restrict
 #pragma unroll
   for (int i = 0; i < 16; ++i) b[i] = 0;
   if (u < npt) {
-    balanced_digits(llrint(ldexp(W[p0 + u], sc->ex[4])), WDIG, b);
+    balanced_digits(llrint(ldexp(W[tile_rows[p0 + u]], sc->ex[4])), WDIG, b);
     b[WDIG] = 1;
   }
   out[128 * t + u] = pack16(b);
@@ -1095,49 +1098,86 @@ struct TcPtrs {
   unsigned long long *mbits, *counters;
   TcScales *sc;
   uint4 *tile_ops;
-  const uint32_t *tile_starts;
+  const uint32_t *tile_starts, *tile_rows;
   const double *tile_boxes;
   double *vals;
   const uint32_t *perm;
 };
 
+// Recursive bisection of the positions idx[b, e) into compact parts:
+// along the longest axis of the part's box, at a multiple of g rows (so that
+// all parts but the last of a branch hold exactly g), until a part holds at
+// most g positions and, when wmax > 0, is at most wmax wide along every axis.
+// Appends each final part's start (depth first: neighbouring parts are
+// neighbours in space) to `cuts` when given.
+void bisect(const double *P, std::vector<uint32_t> &idx, uint32_t b, uint32_t e, uint32_t g,
+            double wmax, std::vector<uint32_t> *cuts) {
+  struct Part {
+    uint32_t b, e;
+  };
+  std::vector<Part> stack{{b, e}};
+  while (!stack.empty()) {
+    const Part t = stack.back();
+    stack.pop_back();
+    const uint32_t n = t.e - t.b;
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = t.b; i < t.e; ++i)
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], P[3 * (size_t)idx[i] + a]);
+        hi[a] = std::max(hi[a], P[3 * (size_t)idx[i] + a]);
+      }
+    int ax = 0;
+    for (int a = 1; a < 3; ++a)
+      if (hi[a] - lo[a] > hi[ax] - lo[ax]) ax = a;
+    const bool wide = wmax > 0 && hi[ax] - lo[ax] > wmax;
+    if (n <= 1 || (n <= g && !wide)) {
+      if (cuts) cuts->push_back(t.b);
+      continue;
+    }
+    uint32_t nl;
+    if (n > g) {
+      nl = g * std::max<uint32_t>(1, (uint32_t)std::lround((double)n / (2.0 * g)));
+      if (nl >= n) nl = g * ((n - 1) / g);
+    } else {
+      nl = n / 2;
+    }
+    std::nth_element(idx.begin() + t.b, idx.begin() + t.b + nl, idx.begin() + t.e,
+                     [&](uint32_t x, uint32_t y) {
+                       const double px = P[3 * (size_t)x + ax], py = P[3 * (size_t)y + ax];
+                       return px != py ? px < py : x < y;
+                     });
+    stack.push_back({t.b + nl, t.e});
+    stack.push_back({t.b, t.b + nl});
+  }
+}
+
 // The tiles of a mesh for a shape radius, kept in the workspace while mesh
-// and radius stay the same: runs of <= 128 consecutive positions (Morton
-// order) within Morton cells of about PRT_TILE_TARGET positions and at most
-// two radii wide (so that a candidate lies within 2 radii of the tile centre
-// along every axis and the score operands stay in FP16 range), with their
+// and radius stay the same: parts of <= 128 positions from recursive
+// bisection, at most two radii wide along every axis (so that a candidate
+// lies within 2 radii of the tile centre along every axis and the score
+// operands stay in FP16 range); inside a tile the rows are bisected again
+// into compact groups of 32 (one per weight warp's rows). With their
 // bounding boxes and the position operands.
 int tc_tiles(const prt_mesh *mesh, prt_workspace *ws, double radius, cudaStream_t s) {
   if (ws->tc_mesh_uid == mesh->uid && ws->tc_radius == radius && ws->tc_tiles > 0)
     return PRT_OK;
   const PositionSet &PS = mesh->positions;
   const long long npos = PS.count;
-  const double ext = mesh->morton_ext;
-  double vol = 1;
-  for (int a = 0; a < 3; ++a) vol *= std::max(mesh->box_hi[a] - mesh->box_lo[a], 1e-300);
-  const double tside = std::cbrt(PRT_TILE_TARGET * vol / std::max<long long>(1, npos));
-  int lt = (int)std::lround(std::log2(ext / tside));
-  int la = (int)std::ceil(std::log2(ext / (2.0 * radius)) + 1e-9);
-  const int level = std::min(std::max(std::max(lt, la), 0), 21);
-  const int shift = 3 * (21 - level);
-  std::vector<uint32_t> ts;
+  const double *P = mesh->pos_host.data();
+  std::vector<uint32_t> rows((size_t)npos), ts;
+  for (long long u = 0; u < npos; ++u) rows[u] = (uint32_t)u;
   ts.reserve(npos / 64 + 2);
-  uint64_t prev = ~0ull;
-  for (long long u = 0; u < npos; ++u) {
-    const uint64_t cell = mesh->pos_key[u] >> shift;
-    if (u == 0 || cell != prev || u - ts.back() >= TM) ts.push_back((uint32_t)u);
-    prev = cell;
-  }
+  bisect(P, rows, 0, (uint32_t)npos, TM, 2.0 * radius * (1 - 1e-9), &ts);
   ts.push_back((uint32_t)npos);
   const long long nt = (long long)ts.size() - 1;
   std::vector<double> tb(6 * (size_t)std::max<long long>(1, nt), 0.0);
-  const double *P = mesh->pos_host.data();
   for (long long t = 0; t < nt; ++t) {
+    bisect(P, rows, ts[t], ts[t + 1], 32, 0.0, nullptr);
     double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (uint32_t u = ts[t]; u < ts[t + 1]; ++u)
+    for (uint32_t i = ts[t]; i < ts[t + 1]; ++i)
       for (int a = 0; a < 3; ++a) {
-        lo[a] = std::min(lo[a], P[3 * (size_t)u + a]);
-        hi[a] = std::max(hi[a], P[3 * (size_t)u + a]);
+        lo[a] = std::min(lo[a], P[3 * (size_t)rows[i] + a]);
+        hi[a] = std::max(hi[a], P[3 * (size_t)rows[i] + a]);
       }
     for (int a = 0; a < 3; ++a) {
       tb[6 * t + a] = 0.5 * (lo[a] + hi[a]);
@@ -1145,17 +1185,19 @@ int tc_tiles(const prt_mesh *mesh, prt_workspace *ws, double radius, cudaStream_
     }
   }
   int rc;
-  const size_t b_ts = align256(4 * (size_t)(nt + 1));
-  char *set = (char *)ws_buffer(ws, PRT_WS_TC_TILESET, b_ts + 48 * (size_t)nt, &rc);
+  const size_t b_ts = align256(4 * (size_t)(nt + 1)), b_tb = align256(48 * (size_t)nt);
+  char *set = (char *)ws_buffer(ws, PRT_WS_TC_TILESET, b_ts + b_tb + 4 * (size_t)npos, &rc);
   if (!set) return rc;
   uint4 *ops = (uint4 *)ws_buffer(ws, PRT_WS_TC_TILES, 4096 * (size_t)nt, &rc);
   if (!ops) return rc;
   // pageable sources: the copies are staged before the calls return
   PRT_CHECK_CUDA(cudaMemcpyAsync(set, ts.data(), 4 * (size_t)(nt + 1), cudaMemcpyHostToDevice, s));
   PRT_CHECK_CUDA(cudaMemcpyAsync(set + b_ts, tb.data(), 48 * (size_t)nt, cudaMemcpyHostToDevice, s));
-  tile_operands_kernel<<<(unsigned)nt, 128, 0, s>>>(nt, (const uint32_t *)set,
-                                                    (const double *)(set + b_ts), PS.pos,
-                                                    1.0 / radius, ops);
+  PRT_CHECK_CUDA(cudaMemcpyAsync(set + b_ts + b_tb, rows.data(), 4 * (size_t)npos,
+                                 cudaMemcpyHostToDevice, s));
+  tile_operands_kernel<<<(unsigned)nt, 128, 0, s>>>(
+      nt, (const uint32_t *)set, (const uint32_t *)(set + b_ts + b_tb),
+      (const double *)(set + b_ts), PS.pos, 1.0 / radius, ops);
   PRT_CHECK_CUDA(cudaGetLastError());
   PRT_CHECK_CUDA(cudaStreamSynchronize(s));
   ws->tc_mesh_uid = mesh->uid;
@@ -1190,11 +1232,12 @@ int tc_buffers(const prt_mesh *mesh, prt_workspace *ws, long long n, TcPtrs &B) 
   B.sc = (TcScales *)(misc + 256);
   B.tile_ops = (uint4 *)ws_buffer(ws, PRT_WS_TC_TILES, 4096 * (size_t)tiles, &rc);
   if (!B.tile_ops) return rc;
-  const size_t b_ts = align256(4 * (size_t)(tiles + 1));
-  char *set = (char *)ws_buffer(ws, PRT_WS_TC_TILESET, b_ts + 48 * (size_t)tiles, &rc);
+  const size_t b_ts = align256(4 * (size_t)(tiles + 1)), b_tb = align256(48 * (size_t)tiles);
+  char *set = (char *)ws_buffer(ws, PRT_WS_TC_TILESET, b_ts + b_tb + 4 * (size_t)PS.count, &rc);
   if (!set) return rc;
   B.tile_starts = (const uint32_t *)set;
   B.tile_boxes = (const double *)(set + b_ts);
+  B.tile_rows = (const uint32_t *)(set + b_ts + b_tb);
   B.vals = (double *)ws_buffer(ws, PRT_WS_DEP_VALUES, 4 * sizeof(double) * PS.count, &rc);
   if (!B.vals) return rc;
   B.perm = (const uint32_t *)ws_buffer(ws, PRT_WS_DEP_VALS, 8 * (size_t)n, &rc);
@@ -1222,12 +1265,13 @@ void tc_args(const prt_mesh *mesh, prt_workspace *ws, prt_shape_function shape,
   A.pay = reinterpret_cast<const double2 *>(ws->buf[PRT_WS_DEP_PARTICLES]);
   A.starts = reinterpret_cast<const uint32_t *>(ws->buf[PRT_WS_DEP_BINSTARTS]);
   A.tile_starts = B.tile_starts;
+  A.tile_rows = B.tile_rows;
   A.tile_boxes = B.tile_boxes;
   A.tile_ops = B.tile_ops;
   A.wdig = nullptr;
   A.cdig = B.cdig;
   A.cpos = B.cpos;
-  A.order = nullptr;  // Morton order: CTAs running together share candidates in L2
+  A.order = nullptr;  // bisection order: CTAs running together share candidates in L2
   A.radius = shape.radius;
   A.inv_radius = 1.0 / shape.radius;
   A.norm_hi = B.nhi;
@@ -1282,7 +1326,8 @@ int tc_charges(const prt_mesh *mesh, prt_workspace *ws, int32_t mode, prt_shape_
     PRT_CHECK_CUDA(cudaGetLastError());
     weight_scale_kernel<<<1, 1, 0, s>>>(B.mbits, kappa, B.sc);
     PRT_CHECK_CUDA(cudaGetLastError());
-    weight_digits_kernel<<<(unsigned)tiles, 128, 0, s>>>(tiles, B.tile_starts, W, B.sc, wdig);
+    weight_digits_kernel<<<(unsigned)tiles, 128, 0, s>>>(tiles, B.tile_starts, B.tile_rows, W,
+                                                         B.sc, wdig);
     PRT_CHECK_CUDA(cudaGetLastError());
     PRT_CHECK_CUDA(cudaMemsetAsync(B.nhi, 0, 8 * (size_t)n, s));
     PRT_CHECK_CUDA(cudaMemsetAsync(B.nlo, 0, 8 * (size_t)n, s));

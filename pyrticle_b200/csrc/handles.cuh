@@ -71,12 +71,9 @@ struct prt_mesh {
   double box_lo[3], box_hi[3];             // node bounding box of the mesh
   PositionSet positions;
   unsigned long long uid = 0;              // unique per created mesh (workspace caches)
-  // host copies of the positions [count][3] and their Morton keys (21 bits
-  // per axis over the cube of side morton_ext at box_lo): the tensor-core
-  // deposition cuts its tiles from them per shape radius
+  // host copy of the positions [count][3]: the tensor-core deposition cuts
+  // its tiles from them per shape radius
   std::vector<double> pos_host;
-  std::vector<uint64_t> pos_key;
-  double morton_ext = 1;
 };
 
 // CUDA-event timing of the main kernels (prt_workspace_timing).
@@ -139,12 +136,6 @@ constexpr double PRT_GROUP_TARGET = 24.0;
 // two sibling cells, about twice the positions)
 #ifndef PRT_WIDE_CELL_BITS
 #define PRT_WIDE_CELL_BITS 1
-#endif
-
-// target positions per Morton cell when cutting the tensor-core tiles (the
-// cells are also at most two shape radii wide)
-#ifndef PRT_TILE_TARGET
-#define PRT_TILE_TARGET 128.0
 #endif
 
 void *ws_buffer(prt_workspace *ws, int slot, size_t bytes, int *rc);
