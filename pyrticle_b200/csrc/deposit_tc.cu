@@ -52,10 +52,12 @@
 //     The tiles are at most two radii wide, so every score operand stays
 //     within FP16 range.
 //
-// Synchronisation per chunk k of a CTA: the score MMA of chunk k runs while
-// the warps stage chunk k+1; the weights of chunk k are written once the
-// accumulation MMA of chunk k-1 has completed (mbarrier); one thread issues
-// the accumulation MMA of chunk k and the score MMA of chunk k+1. Every
+// Synchronisation per chunk k of a CTA: the score MMA of chunk k and the
+// accumulation MMA of chunk k-1 run while the warps stage chunk k+1 (the
+// ring of five chunks holds chunks k-1 .. k+1 and at most 255 slots more);
+// the weights of chunk k are written once the accumulation MMA of chunk k-1
+// has completed (mbarrier); one thread issues the accumulation MMA of chunk k
+// and the score MMA of chunk k+1. Every
 // mbarrier wait is bounded: a CTA whose wait runs out records PRT_ERR_TIMEOUT,
 // stops, waits (bounded) for its issued MMAs and frees its tensor memory.
 
@@ -75,7 +77,7 @@ using namespace prt_dep;
 
 constexpr int TM = 128;          // positions per tile: MMA M, tensor-memory lanes
 constexpr int NC = 128;          // candidates per chunk: score MMA N
-constexpr int RING = 512;        // candidate slots in shared memory
+constexpr int RING = 5 * NC;     // candidate slots in shared memory: five chunks
 constexpr int THREADS = 256;     // eight warps
 constexpr int MAXSEG = 512;      // bin-row segments per tile
 constexpr uint32_t TMEM_COLS = 256;
@@ -104,6 +106,7 @@ struct Smem {
 };
 // 2 CTAs per SM at most (2 x 256 tensor-memory columns = all 512)
 static_assert(sizeof(Smem) + 1024 > 228 * 1024 / 3, "shared memory keeps tensor memory within one SM");
+static_assert(2 * (sizeof(Smem) + 1024) <= 228 * 1024, "two CTAs per SM");
 
 struct TcArgs {
   BinGrid G;
@@ -435,7 +438,7 @@ __device__ __forceinline__ void cursor_init(const Smem &S, const TcArgs &A, Curs
 
 // Stages candidates into the ring until it holds `target` slots or every
 // warp's segments are exhausted (every warp; at most 32 slots per warp past
-// the target).
+// the target, so the ring holds at most target + 255).
 template <bool NORM>
 __device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const double c[3],
                                      const float hf[3], int target, int lane, Cursor &C) {
@@ -472,7 +475,7 @@ __device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const double c[3]
     if (lane == 0 && bal) base = atomicAdd(&S.tail, __popc(bal));
     base = __shfl_sync(0xffffffffu, base, 0);
     if (in) {
-      const int slot = (base + __popc(bal & ((1u << lane) - 1u))) & (RING - 1);
+      const int slot = (base + __popc(bal & ((1u << lane) - 1u))) % RING;
       uint4 k0, k1;
       candidate_operand(w0 * inv_a, w1 * inv_a, w2 * inv_a, k0, k1);
       *reinterpret_cast<uint4 *>(S.bcand + (size_t)slot * 16) = k0;
@@ -502,7 +505,7 @@ __device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const double c[3]
 // tail of the last chunk): a zero operand gives score 0, weight 0.
 __device__ __forceinline__ void pad_chunk(Smem &S, int from, int to, int tid) {
   for (int i = from + tid; i < to; i += THREADS) {
-    const int slot = i & (RING - 1);
+    const int slot = i % RING;
     *reinterpret_cast<uint4 *>(S.bcand + (size_t)slot * 16) = make_uint4(0, 0, 0, 0);
     *reinterpret_cast<uint4 *>(S.bcand + (size_t)(RING + slot) * 16) = make_uint4(0, 0, 0, 0);
     *reinterpret_cast<uint4 *>(S.bdig + (size_t)slot * 16) = make_uint4(0, 0, 0, 0);
@@ -665,7 +668,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
         for (int kk = 0; kk < WDIG; ++kk)
           P += ((__int128)(int)d2[kk] << (8 * kk + 16)) + ((__int128)(int)d1[kk] << (8 * kk + 8)) +
                ((__int128)(int)d0[kk] << (8 * kk));
-        const uint32_t id = S.slot_id[(chunk * NC + cr) & (RING - 1)];
+        const uint32_t id = S.slot_id[(chunk * NC + cr) % RING];
         if (P != 0) {
           // P = H 2^40 + L, 0 <= L < 2^40: both parts add exactly (H modulo 2^64)
           const __int128 H = P >> 40;
@@ -718,7 +721,15 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     if (valid > 0) ++issued_s;
   }
   for (int k = 0; ok && valid > 0; ++k) {
-    // (1) the accumulation of chunk k-1 is complete: its operands may be
+    // (1) stage chunk k+1 while the tensor cores score chunk k and sum chunk
+    // k-1: the fill writes slots of chunks k+1 .. k+3 (at most 255 past
+    // chunk k+1), never those of chunk k-1 (ring of five chunks)
+    fill<NORM>(S, A, c, hf, (k + 2) * NC, lane, cur);
+    __syncthreads();
+    const int valid_next = min(max(S.tail - (k + 1) * NC, 0), NC);
+    if (valid_next > 0 && valid_next < NC)
+      pad_chunk(S, (k + 1) * NC + valid_next, (k + 2) * NC, tid);
+    // (2) the accumulation of chunk k-1 is complete: its weight digits may be
     // overwritten; read the normalisation sums, or fold a full window
     if (k > 0) {
       ok = wait_a();
@@ -731,13 +742,6 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
         window = 0;
       }
     }
-    __syncthreads();
-    // (2) stage chunk k+1 while the tensor cores score chunk k
-    fill<NORM>(S, A, c, hf, (k + 2) * NC, lane, cur);
-    __syncthreads();
-    const int valid_next = min(max(S.tail - (k + 1) * NC, 0), NC);
-    if (valid_next > 0 && valid_next < NC)
-      pad_chunk(S, (k + 1) * NC + valid_next, (k + 2) * NC, tid);
     // (3) the weights of chunk k
     ok = wait_s();
     if (!ok) break;
@@ -749,7 +753,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     // (4) the sums of chunk k, the scores of chunk k+1
     if (tid == 0) {
       fence_after();
-      const int slot0 = (k * NC) & (RING - 1);
+      const int slot0 = (k * NC) % RING;
       if (NORM) {
 #pragma unroll
         for (int d = 0; d < (IND ? FDIG + 1 : FDIG); ++d)
@@ -770,7 +774,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
       }
       mma_commit(bar_a);
       if (valid_next > 0) {
-        const int slot1 = ((k + 1) * NC) & (RING - 1);
+        const int slot1 = ((k + 1) * NC) % RING;
         mma_f16(tmem, sdesc(a_pos, TM * 16, 128), sdesc(b_cand + slot1 * 16, RING * 16, 128),
                 IDESC_SCORE, 0);
         mma_commit(bar_s);
