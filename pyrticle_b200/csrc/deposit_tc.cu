@@ -79,6 +79,8 @@ constexpr int TM = 128;          // positions per tile: MMA M, tensor-memory lan
 constexpr int NC = 128;          // candidates per chunk: score MMA N
 constexpr int RING = 5 * NC;     // candidate slots in shared memory: five chunks
 constexpr int THREADS = 256;     // eight warps
+constexpr int FILL_WARPS = 7;    // warps 0-6 stage candidates
+constexpr int ISSUE_WARP = 7;    // warp 7 issues the tensor-core work
 constexpr int MAXSEG = 512;      // bin-row segments per tile
 constexpr uint32_t TMEM_COLS = 256;
 constexpr uint32_t COL_ACC = 128;  // accumulators: weight digit d at +16 d, indicator at +48
@@ -389,7 +391,7 @@ __device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], cons
 }
 
 // A warp's place in its tile's candidate stream: the warp stages the
-// segments warp, warp + 8, ... of the tile, 32 particles (a batch) at a time,
+// segments warp, warp + FILL_WARPS, ... of the tile, 32 particles (a batch) at a time,
 // with three batches loaded ahead, each in its own registers (a batch's
 // values are read only when it is processed, then the set is refilled).
 struct Batch {
@@ -419,7 +421,7 @@ __device__ __forceinline__ void next_batch(const Smem &S, const TcArgs &A, Curso
   C.coff += 32;
   if (C.coff >= len) {
     C.coff = 0;
-    C.cseg += THREADS / 32;
+    C.cseg += FILL_WARPS;
   }
 }
 
@@ -437,8 +439,8 @@ __device__ __forceinline__ void cursor_init(const Smem &S, const TcArgs &A, Curs
 }
 
 // Stages candidates into the ring until it holds `target` slots or every
-// warp's segments are exhausted (every warp; at most 32 slots per warp past
-// the target, so the ring holds at most target + 255).
+// warp's segments are exhausted (every fill warp; at most 32 slots per warp
+// past the target, so the ring holds at most target + 223).
 template <bool NORM>
 __device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const double c[3],
                                      const float hf[3], int target, int lane, Cursor &C) {
@@ -646,7 +648,12 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   bool ok = S.abort == 0;
   int issued_s = 0, issued_a = 0, waited_s = 0, waited_a = 0;
   Cursor cur;
-  cursor_init<NORM>(S, A, cur, warp, lane);
+  if (warp < FILL_WARPS) {
+    cursor_init<NORM>(S, A, cur, warp, lane);
+  } else {
+    cur.q0.seg = cur.q1.seg = cur.q2.seg = -1;
+    cur.rot = 0;
+  }
   int valid = 0;
 
   // readout of a normalisation chunk: per candidate its sum over the tile
@@ -692,66 +699,77 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     for (int i = 0; i < 8; ++i)
       acc[i] += (double)(65536ll * (int)d2[i] + 256ll * (int)d1[i] + (int)d0[i]);
   };
-  auto wait_s = [&]() {
-    const bool w = mbar_wait(bar_s, (uint32_t)(waited_s & 1));
-    ++waited_s;
-    return __syncthreads_and(w) != 0;
-  };
   auto wait_a = [&]() {
     const bool w = mbar_wait(bar_a, (uint32_t)(waited_a & 1));
-    ++waited_a;
+    if (w) ++waited_a;
     return __syncthreads_and(w) != 0;
   };
+  const bool issuer = warp == ISSUE_WARP && lane == 0;
 
   int window = 0;       // chunks in the current int32 deposition window
   int valid_prev = 0;   // valid slots of the chunk whose accumulation is in flight
   if (ok) {
-    fill<NORM>(S, A, c, hf, NC, lane, cur);
+    if (warp < FILL_WARPS) fill<NORM>(S, A, c, hf, NC, lane, cur);
     __syncthreads();
     valid = min(S.tail, NC);
     if (valid > 0 && valid < NC) pad_chunk(S, valid, NC, tid);
     fence_async_smem();
     fence_before();
     __syncthreads();
-    if (valid > 0 && tid == 0) {
+    if (valid > 0 && issuer) {
       fence_after();
       mma_f16(tmem, sdesc(a_pos, TM * 16, 128), sdesc(b_cand, RING * 16, 128), IDESC_SCORE, 0);
       mma_commit(bar_s);
     }
     if (valid > 0) ++issued_s;
   }
+  // One CTA barrier per chunk: every thread waits for the tensor cores itself
+  // (bounded), and the barrier after the weights joins the fill of chunk
+  // k+1, the weights of chunk k and the waits' outcomes.
   for (int k = 0; ok && valid > 0; ++k) {
-    // (1) stage chunk k+1 while the tensor cores score chunk k and sum chunk
-    // k-1: the fill writes slots of chunks k+1 .. k+3 (at most 255 past
-    // chunk k+1), never those of chunk k-1 (ring of five chunks)
-    fill<NORM>(S, A, c, hf, (k + 2) * NC, lane, cur);
-    __syncthreads();
-    const int valid_next = min(max(S.tail - (k + 1) * NC, 0), NC);
-    if (valid_next > 0 && valid_next < NC)
-      pad_chunk(S, (k + 1) * NC + valid_next, (k + 2) * NC, tid);
+    // (1) the fill warps stage chunk k+1 while the tensor cores score chunk
+    // k and sum chunk k-1: the fill writes slots of chunks k+1 .. k+3 (at
+    // most 223 past chunk k+1), never those of chunk k-1 (ring of five)
+    if (warp < FILL_WARPS) fill<NORM>(S, A, c, hf, (k + 2) * NC, lane, cur);
     // (2) the accumulation of chunk k-1 is complete: its weight digits may be
     // overwritten; read the normalisation sums, or fold a full window
+    bool w = true;
     if (k > 0) {
-      ok = wait_a();
-      if (!ok) break;
-      fence_after();
-      if (NORM) {
-        norm_readout(k - 1, valid_prev);
-      } else if (window == FLUSH_CHUNKS) {
-        dep_fold();
-        window = 0;
+      w = mbar_wait(bar_a, (uint32_t)(waited_a & 1));
+      if (w) {
+        ++waited_a;
+        fence_after();
+        if (NORM) {
+          norm_readout(k - 1, valid_prev);
+        } else if (window == FLUSH_CHUNKS) {
+          dep_fold();
+          window = 0;
+        }
       }
     }
     // (3) the weights of chunk k
-    ok = wait_s();
-    if (!ok) break;
-    fence_after();
-    weights<NORM && IND>(S, tmem, warp, lane);
+    if (w) {
+      w = mbar_wait(bar_s, (uint32_t)(waited_s & 1));
+      if (w) {
+        ++waited_s;
+        fence_after();
+        weights<NORM && IND>(S, tmem, warp, lane);
+      }
+    }
     fence_async_smem();
     fence_before();
-    __syncthreads();
-    // (4) the sums of chunk k, the scores of chunk k+1
-    if (tid == 0) {
+    ok = __syncthreads_and(w) != 0;
+    if (!ok) break;
+    const int valid_next = min(max(S.tail - (k + 1) * NC, 0), NC);
+    if (valid_next > 0 && valid_next < NC) {
+      // the stream ends inside chunk k+1: zero its remaining slots
+      pad_chunk(S, (k + 1) * NC + valid_next, (k + 2) * NC, tid);
+      fence_async_smem();
+      __syncthreads();
+    }
+    // (4) the sums of chunk k, the scores of chunk k+1 (the issue warp; the
+    // fill warps go on to chunk k+2)
+    if (issuer) {
       fence_after();
       const int slot0 = (k * NC) % RING;
       if (NORM) {
