@@ -93,18 +93,20 @@ constexpr int CDIG = 6, JDIG = 3, WDIG = 6;
 struct Smem {
   uint8_t apos[2 * TM * 16];     // position operand, K-major: [K chunk][row][16 B]
   uint8_t bcand[2 * RING * 16];  // candidate operands, K-major: [K chunk][slot][16 B]
-  uint8_t bdig[RING * 16];       // charge digits per slot (16 columns, MN-major)
+  union {
+    uint8_t bdig[RING * 16];     // deposition: charge digits per slot (16 columns, MN-major)
+    uint32_t slot_id[RING];      // normalisation: bin-order particle of a slot
+  };
   uint8_t wdig[TM * 16];         // weight digits per position (16 columns, MN-major)
   // weight digits: [byte 2, byte 1, byte 0, indicator][16-candidate block][position][16 B]
   uint8_t fdig[FDIG + 1][NC / 16][TM][16];
-  uint32_t slot_id[RING];        // bin-order particle of a slot (normalisation)
-  uint32_t seg_start[MAXSEG];    // first bin-order particle of a segment
-  uint32_t seg_pref[MAXSEG + 1]; // stream offset of a segment
-  uint8_t seg_img[MAXSEG];       // periodic image (qx+1) + 3 (qy+1) + 9 (qz+1)
-  uint32_t seg_row[MAXSEG];      // bin row of a segment: wy | wz << 16
+  // per segment: the origin of its first bin relative to the tile centre
+  // (periodic image included) and that bin's x index
+  float4 seg_o[MAXSEG];
+  uint2 seg_sl[MAXSEG];          // per segment: first bin-order particle, length
   unsigned long long bar_s, bar_a;
   uint32_t tmem;
-  int tail, cursor, nseg, total, abort;
+  int tail, nseg, abort;
 };
 // 2 CTAs per SM at most (2 x 256 tensor-memory columns = all 512)
 static_assert(sizeof(Smem) + 1024 > 228 * 1024 / 3, "shared memory keeps tensor memory within one SM");
@@ -121,7 +123,7 @@ struct TcArgs {
   const uint4 *__restrict__ wdig;       // [tiles][128] weight digits
   const uint4 *__restrict__ cdig;       // [n] charge digits, bin order
   // [n] bin order: position relative to the particle's bin origin (FP32)
-  // and the bin's x index (int bits)
+  // and the bin's x index (as a float: exact)
   const float4 *__restrict__ cpos;
   const uint32_t *__restrict__ order;   // launch order of the tiles (or NULL)
   double radius, inv_radius;
@@ -267,8 +269,10 @@ __device__ __forceinline__ void candidate_operand(float w0, float w1, float w2, 
 
 // Bin-row segments of a tile (warp 0): every run of bins along x, in the
 // rows (bz, by) within the radius of the box [c - hf, c + hf], as ranges of
-// bin-order particles with their periodic image; the stream of candidates
-// is the concatenation of the segments.
+// bin-order particles with the origin of the run's first bin relative to the
+// tile centre (periodic image included, FP64 rounded once to FP32: within
+// 2.5 radii, so to ~2e-7 radii); the stream of candidates is the
+// concatenation of the segments.
 __device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], const double hf[3],
                                int lane) {
   const BinGrid &G = A.G;
@@ -294,14 +298,12 @@ __device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], cons
   const int ny = max(0, uhi[1] - ulo[1] + 1), nz = max(0, uhi[2] - ulo[2] + 1);
   const int nrows = ny * nz;
   int nseg = 0;
-  uint32_t total = 0;
   bool overflow = false;
   for (int r0 = 0; r0 < nrows; r0 += 32) {
     const int r = r0 + lane;
-    uint32_t s_start[3], s_len[3], s_row = 0;
-    uint8_t s_img[3];
+    uint32_t s_start[3], s_len[3];
+    float s_ox[3], s_bx[3], oy = 0, oz = 0;
     int cnt = 0;
-    uint32_t len = 0;
     if (r < nrows) {
       const int bz = ulo[2] + r / ny, by = ulo[1] + r % ny;
       int wz = bz, qz = 0, wy = by, qy = 0;
@@ -326,7 +328,8 @@ __device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], cons
         bx0 = max(bx0, ulo[0]);
         bx1 = min(bx1, uhi[0]);
         const long long row = (long long)G.dims[0] * (wy + (long long)G.dims[1] * wz);
-        s_row = (uint32_t)wy | ((uint32_t)wz << 16);
+        oy = (float)(G.origin[1] + wy * G.w[1] + qy * G.period[1] - c[1]);
+        oz = (float)(G.origin[2] + wz * G.w[2] + qz * G.period[2] - c[2]);
         int bx = bx0;
         while (bx <= bx1) {
           int wx = bx, qx = 0, seg_end = bx1;
@@ -342,8 +345,8 @@ __device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], cons
             if (cnt < 3) {
               s_start[cnt] = s0;
               s_len[cnt] = s1 - s0;
-              s_img[cnt] = (uint8_t)((qx + 1) + 3 * (qy + 1) + 9 * (qz + 1));
-              len += s1 - s0;
+              s_ox[cnt] = (float)(G.origin[0] + wx * G.w[0] + qx * G.period[0] - c[0]);
+              s_bx[cnt] = (float)wx;
               ++cnt;
             } else {
               overflow = true;
@@ -352,37 +355,25 @@ __device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], cons
         }
       }
     }
-    // exclusive warp scans of the segment counts and lengths
+    // exclusive warp scan of the segment counts
     int cs = cnt;
-    uint32_t ls = len;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int c2 = __shfl_up_sync(0xffffffffu, cs, o);
-      const uint32_t l2 = __shfl_up_sync(0xffffffffu, ls, o);
-      if (lane >= o) {
-        cs += c2;
-        ls += l2;
-      }
+      if (lane >= o) cs += c2;
     }
     const int sbase = nseg + cs - cnt;
-    uint32_t lbase = total + ls - len;
     for (int i = 0; i < cnt; ++i) {
       if (sbase + i < MAXSEG) {
-        S.seg_start[sbase + i] = s_start[i];
-        S.seg_pref[sbase + i] = lbase;
-        S.seg_img[sbase + i] = s_img[i];
-        S.seg_row[sbase + i] = s_row;
+        S.seg_sl[sbase + i] = make_uint2(s_start[i], s_len[i]);
+        S.seg_o[sbase + i] = make_float4(s_ox[i], oy, oz, s_bx[i]);
       }
-      lbase += s_len[i];
     }
     nseg += __shfl_sync(0xffffffffu, cs, 31);
-    total += __shfl_sync(0xffffffffu, ls, 31);
   }
   overflow = __any_sync(0xffffffffu, overflow) || nseg > MAXSEG;
   if (lane == 0) {
     S.nseg = overflow ? 0 : nseg;
-    S.total = overflow ? 0 : (int)total;
-    S.seg_pref[overflow ? 0 : nseg] = overflow ? 0 : total;
     if (overflow) {
       S.abort = 1;
       record_error(A.st, PRT_ERR_CAPACITY, -1);
@@ -395,13 +386,16 @@ __device__ void build_segments(Smem &S, const TcArgs &A, const double c[3], cons
 // with three batches loaded ahead, each in its own registers (a batch's
 // values are read only when it is processed, then the set is refilled).
 struct Batch {
-  int seg, off;  // seg < 0: none
+  int seg;       // seg < 0: none
+  int n;         // particles of the batch (lanes 0 .. n-1)
+  uint32_t k0;   // bin-order index of lane 0's particle
   float4 pos;    // the lane's particle: offset from its bin origin, bin x index
   uint4 dig;     // its charge digits (deposition pass)
 };
 
 struct Cursor {
   int cseg, coff;  // the next batch to load
+  int nseg;        // segments of the tile
   int rot;         // the set that holds the oldest loaded batch
   Batch q0, q1, q2;
 };
@@ -409,17 +403,18 @@ struct Cursor {
 template <bool NORM>
 __device__ __forceinline__ void next_batch(const Smem &S, const TcArgs &A, Cursor &C, Batch &B,
                                            int lane) {
-  B.seg = C.cseg < S.nseg ? C.cseg : -1;
-  B.off = C.coff;
+  B.seg = C.cseg < C.nseg ? C.cseg : -1;
   if (B.seg < 0) return;
-  const int len = (int)(S.seg_pref[B.seg + 1] - S.seg_pref[B.seg]);
-  if (B.off + lane < len) {
-    const size_t k = (size_t)S.seg_start[B.seg] + B.off + lane;
+  const uint2 sl = S.seg_sl[B.seg];
+  B.n = (int)sl.y - C.coff;
+  B.k0 = sl.x + (uint32_t)C.coff;
+  if (lane < B.n) {
+    const size_t k = (size_t)B.k0 + lane;
     B.pos = A.cpos[k];
     if (!NORM) B.dig = A.cdig[k];
   }
   C.coff += 32;
-  if (C.coff >= len) {
+  if (C.coff >= (int)sl.y) {
     C.coff = 0;
     C.cseg += FILL_WARPS;
   }
@@ -430,6 +425,7 @@ __device__ __forceinline__ void cursor_init(const Smem &S, const TcArgs &A, Curs
                                             int lane) {
   C.cseg = warp;
   C.coff = 0;
+  C.nseg = S.nseg;
   C.rot = 0;
   C.q0.pos = C.q1.pos = C.q2.pos = make_float4(0, 0, 0, 0);
   C.q0.dig = C.q1.dig = C.q2.dig = make_uint4(0, 0, 0, 0);
@@ -442,31 +438,25 @@ __device__ __forceinline__ void cursor_init(const Smem &S, const TcArgs &A, Curs
 // warp's segments are exhausted (every fill warp; at most 32 slots per warp
 // past the target, so the ring holds at most target + 223).
 template <bool NORM>
-__device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const double c[3],
-                                     const float hf[3], int target, int lane, Cursor &C) {
-  const BinGrid &G = A.G;
+__device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const float hf[3], int target,
+                                     int lane, Cursor &C) {
   const float rcf = (float)(A.radius * (1 + 1e-5));
   const float rc4 = 4.0f * rcf * rcf;
   const float inv_a = (float)A.inv_radius;
+  const float bw = (float)A.G.w[0];
   // culls batch B into the ring, then refills B with the warp's next batch
   auto process = [&](Batch &B) {
-    const int len = (int)(S.seg_pref[B.seg + 1] - S.seg_pref[B.seg]);
-    const bool valid = B.off + lane < len;
-    const uint32_t k = S.seg_start[B.seg] + (uint32_t)(B.off + lane);
-    const int img = S.seg_img[B.seg];
-    const uint32_t brow = S.seg_row[B.seg];
-    // bin origins relative to the tile centre (FP64), periodic image included
-    const double ox = G.origin[0] + (img % 3 - 1) * G.period[0] - c[0];
-    const float oy = (float)(G.origin[1] + (double)(brow & 0xffffu) * G.w[1] +
-                             ((img / 3) % 3 - 1) * G.period[1] - c[1]);
-    const float oz = (float)(G.origin[2] + (double)(brow >> 16) * G.w[2] +
-                             (img / 9 - 1) * G.period[2] - c[2]);
+    const bool valid = lane < B.n;
+    const uint32_t k = B.k0 + (uint32_t)lane;
+    // the particle relative to the tile centre: its segment's first bin
+    // origin, whole bins along x to its own bin, its offset in the bin
+    const float4 o = S.seg_o[B.seg];
     bool in = false;
     float w0 = 0, w1 = 0, w2 = 0;
     if (valid) {
-      w0 = (float)fma((double)__float_as_int(B.pos.w), G.w[0], ox) + B.pos.x;
-      w1 = oy + B.pos.y;
-      w2 = oz + B.pos.z;
+      w0 = fmaf(B.pos.w - o.w, bw, o.x) + B.pos.x;
+      w1 = o.y + B.pos.y;
+      w2 = o.z + B.pos.z;
       // rounded-box cull: per axis 2 max(|w| - half, 0) = d + |d|
       const float d0 = fabsf(w0) - hf[0], d1 = fabsf(w1) - hf[1], d2 = fabsf(w2) - hf[2];
       const float e0 = d0 + fabsf(d0), e1 = d1 + fabsf(d1), e2 = d2 + fabsf(d2);
@@ -616,7 +606,6 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.bar_a)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     S.tail = 0;
-    S.cursor = 0;
     S.abort = 0;
   }
   {
@@ -709,7 +698,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   int window = 0;       // chunks in the current int32 deposition window
   int valid_prev = 0;   // valid slots of the chunk whose accumulation is in flight
   if (ok) {
-    if (warp < FILL_WARPS) fill<NORM>(S, A, c, hf, NC, lane, cur);
+    if (warp < FILL_WARPS) fill<NORM>(S, A, hf, NC, lane, cur);
     __syncthreads();
     valid = min(S.tail, NC);
     if (valid > 0 && valid < NC) pad_chunk(S, valid, NC, tid);
@@ -730,7 +719,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     // (1) the fill warps stage chunk k+1 while the tensor cores score chunk
     // k and sum chunk k-1: the fill writes slots of chunks k+1 .. k+3 (at
     // most 223 past chunk k+1), never those of chunk k-1 (ring of five)
-    if (warp < FILL_WARPS) fill<NORM>(S, A, c, hf, (k + 2) * NC, lane, cur);
+    if (warp < FILL_WARPS) fill<NORM>(S, A, hf, (k + 2) * NC, lane, cur);
     // (2) the accumulation of chunk k-1 is complete: its weight digits may be
     // overwritten; read the normalisation sums, or fold a full window
     bool w = true;
@@ -867,7 +856,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
 
 // The candidates' compact positions (bin order): the offset from the
 // particle's bin origin in FP32 (below a bin width: exact to ~1e-7 of it) and
-// the bin's x index.
+// the bin's x index (a float, exact).
 __global__ void candidate_positions_kernel(long long n, const uint32_t *__restrict__ perm,
                                            const double *__restrict__ x, BinGrid G,
                                            float4 *__restrict__ out) {
@@ -883,7 +872,7 @@ __global__ void candidate_positions_kernel(long long n, const uint32_t *__restri
     d[a] = (float)(xa - (G.origin[a] + b * G.w[a]));
     if (a == 0) b0 = b;
   }
-  out[s] = make_float4(d[0], d[1], d[2], __int_as_float(b0));
+  out[s] = make_float4(d[0], d[1], d[2], (float)b0);
 }
 
 // Position operands of every tile, K-major: row u of tile t at
