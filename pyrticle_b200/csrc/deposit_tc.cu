@@ -1182,6 +1182,7 @@ int tc_tiles(const prt_mesh *mesh, prt_workspace *ws, double radius, cudaStream_
   ts.push_back((uint32_t)npos);
   const long long nt = (long long)ts.size() - 1;
   std::vector<double> tb(6 * (size_t)std::max<long long>(1, nt), 0.0);
+  double hf_max = 0;
   for (long long t = 0; t < nt; ++t) {
     bisect(P, rows, ts[t], ts[t + 1], 32, 0.0, nullptr);
     double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -1193,7 +1194,20 @@ int tc_tiles(const prt_mesh *mesh, prt_workspace *ws, double radius, cudaStream_
     for (int a = 0; a < 3; ++a) {
       tb[6 * t + a] = 0.5 * (lo[a] + hi[a]);
       tb[6 * t + 3 + a] = 0.5 * (hi[a] - lo[a]);
+      hf_max = std::max(hf_max, tb[6 * t + 3 + a]);
     }
+  }
+  // particle bins a quarter radius wide (the bin rows that a tile stages hold
+  // ~1.4 times the particles within the radius of its box; half-radius bins
+  // ~1.9 times), wider where a tile's segments could exceed MAXSEG: per axis
+  // at most (2 hf + 2 a) / w + 4 bin rows, a row in at most three pieces
+  // along a periodic x
+  const bool per_x = mesh->dev.pmin[0] != mesh->dev.pmax[0];
+  double bw = 0.25 * radius;
+  for (;;) {
+    const double rows = (2 * hf_max + 2 * radius) / bw + 4;
+    if (rows * rows * (per_x ? 3 : 1) <= MAXSEG) break;
+    bw *= 1.125;
   }
   int rc;
   const size_t b_ts = align256(4 * (size_t)(nt + 1)), b_tb = align256(48 * (size_t)nt);
@@ -1214,6 +1228,7 @@ int tc_tiles(const prt_mesh *mesh, prt_workspace *ws, double radius, cudaStream_
   ws->tc_mesh_uid = mesh->uid;
   ws->tc_radius = radius;
   ws->tc_tiles = nt;
+  ws->tc_bin_width = bw;
   return PRT_OK;
 }
 
@@ -1257,10 +1272,12 @@ int tc_buffers(const prt_mesh *mesh, prt_workspace *ws, long long n, TcPtrs &B) 
   return PRT_OK;
 }
 
-int tc_bins(const prt_mesh *mesh, prt_shape_function shape, BinGrid &G) {
+// The particle bins of the tensor-core deposition (after tc_tiles): the
+// width the tiles chose.
+int tc_bins(const prt_mesh *mesh, const prt_workspace *ws, prt_shape_function shape,
+            BinGrid &G) {
   int rc;
-  if (!choose_bins(mesh, mesh->box_lo, mesh->box_hi, shape.radius * BIN_FRACTION, shape.radius,
-                   G, &rc))
+  if (!choose_bins(mesh, mesh->box_lo, mesh->box_hi, ws->tc_bin_width, shape.radius, G, &rc))
     return rc;
   return PRT_OK;
 }
@@ -1305,8 +1322,8 @@ int tc_charges(const prt_mesh *mesh, prt_workspace *ws, int32_t mode, prt_shape_
   const PositionSet &PS = mesh->positions;
   const bool norm = mode == PRT_DEPOSIT_NORMALIZED;
   int rc;
-  if ((rc = tc_bins(mesh, shape, G))) return rc;
   if ((rc = tc_tiles(mesh, ws, shape.radius, s))) return rc;
+  if ((rc = tc_bins(mesh, ws, shape, G))) return rc;
   const long long tiles = ws->tc_tiles;
   if ((rc = tc_buffers(mesh, ws, n, B))) return rc;
   const double kappa = tc_kappa(shape);
@@ -1451,7 +1468,7 @@ extern "C" int prt_deposit_shape_sums(const prt_mesh *mesh, prt_workspace *ws,
   TcPtrs B;
   BinGrid G;
   int rc;
-  if ((rc = tc_bins(mesh, shape, G))) return rc;
+  if ((rc = tc_bins(mesh, ws, shape, G))) return rc;
   if ((rc = tc_buffers(mesh, ws, n, B))) return rc;
   return tc_deposit(mesh, ws, shape, n, G, B, global_max, sums, s);
 }

@@ -94,6 +94,7 @@ struct prt_workspace {
   unsigned long long tc_mesh_uid = 0;
   double tc_radius = 0;
   long long tc_tiles = 0;   // tiles of that mesh and radius (PRT_WS_TC_TILESET)
+  double tc_bin_width = 0;  // particle bin width for those tiles
   long long tc_n = -1;      // particles of the last tensor-core charges step
   DevStatus *status = nullptr;
   bool timing = false;
