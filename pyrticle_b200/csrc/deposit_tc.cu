@@ -56,8 +56,8 @@
 // accumulation MMA of chunk k-1 run while the warps stage chunk k+1 (the
 // ring of five chunks holds chunks k-1 .. k+1 and at most 255 slots more);
 // the weights of chunk k are written once the accumulation MMA of chunk k-1
-// has completed (mbarrier); one thread issues the accumulation MMA of chunk k
-// and the score MMA of chunk k+1. Every
+// has completed (mbarrier); one thread of a warp that stages nothing issues
+// the score MMA of chunk k+1 and the accumulation MMA of chunk k. Every
 // mbarrier wait is bounded: a CTA whose wait runs out records PRT_ERR_TIMEOUT,
 // stops, waits (bounded) for its issued MMAs and frees its tensor memory.
 
@@ -756,10 +756,16 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
       fence_async_smem();
       __syncthreads();
     }
-    // (4) the sums of chunk k, the scores of chunk k+1 (the issue warp; the
-    // fill warps go on to chunk k+2)
+    // (4) the scores of chunk k+1, then the sums of chunk k (the issue warp;
+    // the fill warps go on to chunk k+2)
     if (issuer) {
       fence_after();
+      if (valid_next > 0) {
+        const int slot1 = ((k + 1) * NC) % RING;
+        mma_f16(tmem, sdesc(a_pos, TM * 16, 128), sdesc(b_cand + slot1 * 16, RING * 16, 128),
+                IDESC_SCORE, 0);
+        mma_commit(bar_s);
+      }
       const int slot0 = (k * NC) % RING;
       if (NORM) {
 #pragma unroll
@@ -780,12 +786,6 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
                    (window > 0 || jj > 0) ? 1u : 0u);
       }
       mma_commit(bar_a);
-      if (valid_next > 0) {
-        const int slot1 = ((k + 1) * NC) % RING;
-        mma_f16(tmem, sdesc(a_pos, TM * 16, 128), sdesc(b_cand + slot1 * 16, RING * 16, 128),
-                IDESC_SCORE, 0);
-        mma_commit(bar_s);
-      }
     }
     ++issued_a;
     if (valid_next > 0) ++issued_s;
