@@ -645,32 +645,37 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   }
   int valid = 0;
 
-  // readout of a normalisation chunk: per candidate its sum over the tile
+  // readout of a normalisation chunk: per candidate its sum over the tile,
+  // P = H 2^40 + L (0 <= L < 2^40), both parts added exactly to the
+  // particle's integral (H modulo 2^64): warps 0-3 add H, warps 4-7 add L and
+  // the hit count (a warp reads the tensor-memory lanes 32 (warp % 4) ..)
   auto norm_readout = [&](int chunk, int nvalid) {
-    if (warp < 4) {
-      uint32_t d2[8], d1[8], d0[8], di[8];
-      const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
-      tmem_ld8(lane_addr + COL_ACC, d2);
-      tmem_ld8(lane_addr + COL_ACC + 16, d1);
-      tmem_ld8(lane_addr + COL_ACC + 32, d0);
-      if (IND) tmem_ld8(lane_addr + COL_ACC + 48, di);
-      tmem_wait_ld();
-      const int cr = 32 * warp + lane;
-      if (cr < nvalid) {
-        // the tile's part of the integral, exactly:
-        // sum_kk 256^kk (65536 D2 + 256 D1 + D0)
-        __int128 P = 0;
+    uint32_t d2[8], d1[8], d0[8], di[8];
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+    tmem_ld8(lane_addr + COL_ACC, d2);
+    tmem_ld8(lane_addr + COL_ACC + 16, d1);
+    tmem_ld8(lane_addr + COL_ACC + 32, d0);
+    if (IND && warp >= 4) tmem_ld8(lane_addr + COL_ACC + 48, di);
+    tmem_wait_ld();
+    const int cr = 32 * (warp & 3) + lane;
+    if (cr < nvalid) {
+      // e_kk = 65536 D2 + 256 D1 + D0 (|e| < 2^38) for the six W digits kk:
+      // P = sum_kk 256^kk e_kk = Plo + 2^24 Phi (|Plo|, |Phi| < 2^55)
+      long long e[WDIG];
 #pragma unroll
-        for (int kk = 0; kk < WDIG; ++kk)
-          P += ((__int128)(int)d2[kk] << (8 * kk + 16)) + ((__int128)(int)d1[kk] << (8 * kk + 8)) +
-               ((__int128)(int)d0[kk] << (8 * kk));
-        const uint32_t id = S.slot_id[(chunk * NC + cr) % RING];
-        if (P != 0) {
-          // P = H 2^40 + L, 0 <= L < 2^40: both parts add exactly (H modulo 2^64)
-          const __int128 H = P >> 40;
-          atomicAdd(A.norm_hi + id, (unsigned long long)(long long)H);
-          atomicAdd(A.norm_lo + id, (unsigned long long)(P - (H << 40)));
-        }
+      for (int kk = 0; kk < WDIG; ++kk)
+        e[kk] = 65536ll * (int)d2[kk] + 256ll * (int)d1[kk] + (long long)(int)d0[kk];
+      const long long plo = e[0] + e[1] * 256 + e[2] * 65536;
+      const long long phi = e[3] + e[4] * 256 + e[5] * 65536;
+      const long long M40 = (1ll << 40) - 1;
+      const long long l1 = (plo & M40) + ((phi & 0xffff) << 24);  // < 2^41
+      const long long L = l1 & M40;
+      const long long H = (plo >> 40) + (phi >> 16) + (l1 >> 40);
+      const uint32_t id = S.slot_id[(chunk * NC + cr) % RING];
+      if (warp < 4) {
+        if (H != 0) atomicAdd(A.norm_hi + id, (unsigned long long)H);
+      } else {
+        if (L != 0) atomicAdd(A.norm_lo + id, (unsigned long long)L);
         if (IND && di[WDIG]) atomicAdd(A.hits + id, di[WDIG]);
       }
     }
