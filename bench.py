@@ -646,9 +646,9 @@ def main():
     avg_norm = nms / max(nk, 1)
     # executed tensor work per evaluated (position, particle) pair in dense
     # FP16 equivalents: the score, 2 x 16 (kind::f16, K = 16); the sums,
-    # 2 weight digits x 16 columns x 2 int8 ops counted at half (the int8
+    # 3 weight digits x 16 columns x 2 int8 ops counted at half (the int8
     # rate is twice the FP16 rate)
-    tensor_per_pair = 32 + 32
+    tensor_per_pair = 32 + 48
     achieved = tensor_per_pair * evaluated_tc / (avg_gather * 1e-3) / 1e12
     useful = 15.0 * pairs / (avg_gather * 1e-3) / 1e12
     gms64, gk64 = kernel64["deposit_gather"]
@@ -698,7 +698,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f16/i8 tensor + f32 + f64 (mixed: split-FP16 tensor-core shape scores, "
-                     "16-bit integer weights summed exactly on the int8 tensor cores, FP64 "
+                     "23-bit integer weights (three digits) summed exactly on the int8 tensor cores, FP64 "
                      "per-node combine and normalisation; split-BF16 tensor-core Lagrange "
                      "values; FP64 state/force/locate)",
             "data": "synthetic (seeded mesh, particles and fields of the workload)",
