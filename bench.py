@@ -154,6 +154,27 @@ def timing_read(m, cat, reset=True):
     return ms.value, k.value
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
+# dominant kernels on the config2 workload at full size (16M particles), from
+# one-pass ncu captures of `python bench.py --steps 1 --warmup 1 --no-e2e
+# --no-adjoint --no-cpu-baseline` (summarised in
+# profiles/dram_traffic_config2_16M.md); reported only for that workload.
+MEASURED_TRAFFIC = {
+    "config2": {
+        "tc_deposit_kernel<0, 0>": 1482749952 + 120223488,
+        "tc_deposit_kernel<1, 1>": 1080907008 + 523428096,
+        "deposit_groups_kernel<1, 1, 2>": 166834674176 + 130093312,
+        "lsrk_stage_mixed_kernel<3>": 2012872448 + 1545450240,
+    }
+}
+
+
+def measured_traffic(args, kernel):
+    if args.scale != 1.0:
+        return None
+    return MEASURED_TRAFFIC.get(args.workload, {}).get(kernel)
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -663,7 +684,8 @@ def main():
     roofline = {"bound": "tensor",
                 "kernel": "tc_deposit_kernel (deposition pass, chosen form)",
                 "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
-                "traffic": None,
+                "traffic": measured_traffic(args, "tc_deposit_kernel<0, 0>"),
+                "traffic_normalize_pass": measured_traffic(args, "tc_deposit_kernel<1, 1>"),
                 "peak_source": ("MEASURED_PEAKS.json bf16_tflops" if src == "measured" else
                                 "fallback 1,590 TFLOP/s (dense BF16, this pool)"),
                 "algorithmic": (f"{tensor_per_pair} dense-FP16-equivalent tensor flops per "
@@ -681,6 +703,7 @@ def main():
                 "secondary": {"bound": "hbm", "kernel": "lsrk_stage_mixed_kernel<3>",
                               "achieved": stage_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                               "frac": stage_gbs / peaks["hbm_gbs"],
+                              "traffic": measured_traffic(args, "lsrk_stage_mixed_kernel<3>"),
                               "algorithmic": "216 B per particle per stage",
                               "peak_source": src}}
     fp64_block = {
@@ -688,7 +711,8 @@ def main():
         "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kernel64.items()},
         "roofline": {"bound": "fp64", "kernel": "deposit_groups_kernel (deposition, FP64)",
                      "achieved": achieved64, "peak": fp64, "unit": "TFLOP/s",
-                     "frac": achieved64 / fp64, "traffic": None,
+                     "frac": achieved64 / fp64,
+                     "traffic": measured_traffic(args, "deposit_groups_kernel<1, 1, 2>"),
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
                      "algorithmic": algorithmic + f"; {avg_gather64:.3f} ms per launch"},
         "form": ("plain form: FP64 throughout" +
