@@ -526,6 +526,106 @@ def adjoint_bench(torch, scale, hbm_gbs, reps=3, checkpoint_every=10):
                                                          torch.linalg.norm(sqt64))}}
 
 
+def grid_bench(args, torch):
+    """config1: GridDepositor (shape weights on one 128 x 128 x 512 brick's
+    points, then the remap to the DG nodes; FP64), 4M particles, order 3,
+    radius 0.1 cm. Times the host set-up, and K steps of the FP64 form and of
+    the mixed form (tensor-core stages; the grid deposition is FP64 in both).
+    One GPU only."""
+    from pyrticle_b200 import problems
+    from pyrticle_b200.cloud import PicMethod
+    from pyrticle_b200.deposition.grid import GridDepositor
+    from pyrticle_b200.deposition.grid_base import SingleBrickGenerator
+    from pyrticle_b200.discretization import Discretization
+    from pyrticle_b200.pusher import MonomialParticlePusher
+    from pyrticle_b200.tools import PolynomialShapeFunction
+    from pyrticle_b200.units import SIUnitsWithNaturalConstants as U
+    w = problems.make("config1", scale=args.scale)
+    discr = Discretization(w.mesh, w.order, nodes=w.nodes)
+    t0 = time.perf_counter()
+    dep = GridDepositor(SingleBrickGenerator(dims=w.brick_dims))
+    m = PicMethod(discr, U, dep, MonomialParticlePusher(), 3, 3)
+    setup_s = time.perf_counter() - t0
+    sf = PolynomialShapeFunction(w.shape_radius, 3, 2)
+    m.depositor.set_shape_function(None, sf)
+    s = m.make_state()
+    m.add_particles_from_arrays(s, w.positions, w.momenta, w.charges, w.masses)
+    fields = torch.as_tensor(w.fields, device="cuda")
+    n = len(s)
+
+    def one_step(prec):
+        return m.step(s, fields, w.dt, steps=1, check=False, precision=prec)
+
+    for prec in (0, 1):
+        for _ in range(args.warmup):
+            one_step(prec)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+
+    def timed(prec):
+        _lib_check = m.lib.prt_workspace_timing
+        _lib_check(m.workspace, 1)
+        for cat in range(7):
+            timing_read(m, cat, reset=True)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        e[0].record()
+        for _ in range(args.steps):
+            one_step(prec)
+        e[1].record()
+        torch.cuda.synchronize()
+        _lib_check(m.workspace, 0)
+        kernel = {name: timing_read(m, cat)[0] / args.steps for cat, name in
+                  ((0, "deposit_grid"), (1, "deposit_stage"), (2, "lsrk_stage"), (3, "sort"))}
+        return e[0].elapsed_time(e[1]), kernel
+
+    ms64, k64 = timed(0)
+    ms, k = timed(1)
+    clk = clocks.stop()
+    m.check_status()
+    # the remap alone (rho and the three j components), CUDA events
+    gr, gj = dep.deposit_grid_densities_device(s)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    e[0].record()
+    dep.remap_grid_to_mesh_device(gr)
+    dep.remap_grid_to_mesh_device(gj)
+    e[1].record()
+    torch.cuda.synchronize()
+    remap_ms = e[0].elapsed_time(e[1])
+    # algorithmic work of the grid deposition: 15 flops per (particle, grid
+    # point) pair within the radius, the points of a radius ball
+    cell = float(np.prod(np.asarray(dep.bricks[0].stepwidths)))
+    pairs = n * (4.0 / 3.0 * np.pi * sf.radius ** 3) / cell
+    fp64 = fp64_peak_tflops(torch)
+    achieved = 15.0 * pairs / (k64["deposit_grid"] * 1e-3) / 1e12
+    value = n * args.steps / (ms * 1e-3)
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 grid deposition and remap; mixed stages (split-BF16 tensor-core "
+                     "Lagrange values, FP64 state/force/locate)",
+            "data": "synthetic (seeded mesh, particles and fields of the workload)",
+            "config": {"workload": f"config1: {w.mesh.element_count} tets order {w.order}, "
+                                   f"{n} particles, GridDepositor on one "
+                                   f"{'x'.join(str(d) for d in w.brick_dims)} brick, shape "
+                                   f"radius {sf.radius * 100:g} cm",
+                       "particles_per_gpu": n, "grid_points": dep.grid_node_count,
+                       "l2": "inputs larger than L2", "parallelism": "1 GPU"},
+            "clocks": clk, "e2e": None,
+            "grid_setup_s": setup_s,
+            "kernel_ms_per_step": k, "remap_ms_per_deposition": remap_ms,
+            "fp64": {"value": n * args.steps / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
+                     "kernel_ms_per_step": k64},
+            "roofline": {"bound": "fp64", "kernel": "deposit_grid_kernel (FP64)",
+                         "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+                         "frac": achieved / fp64, "traffic": None,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                         "algorithmic": f"15 flops x {pairs:.4g} (particle, grid point) pairs "
+                                        "within the radius per deposition"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -534,6 +634,9 @@ def main():
     import torch
     import torch.distributed as dist
 
+    if args.workload == "config1":
+        grid_bench(args, torch)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -564,6 +564,7 @@ extern "C" int prt_deposit_grid(const prt_grid *g, prt_workspace *ws, int32_t we
   T.check_tag = weights == PRT_GRID_TRILINEAR;
   if (grid_rho) PRT_CHECK_CUDA(cudaMemsetAsync(grid_rho, 0, G_n * sizeof(double), s));
   if (grid_j) PRT_CHECK_CUDA(cudaMemsetAsync(grid_j, 0, 3 * G_n * sizeof(double), s));
+  ScopedTimer timer(ws, PRT_TIME_DEPOSIT_GATHER, s);
   if (weights == PRT_GRID_TRILINEAR)
     deposit_grid_kernel<BrickTarget, W_TRILINEAR><<<(unsigned)g->tiles, BLOCK, 0, s>>>(
         T, G, P, S, grid_rho, grid_j, G_n, g->bricks, nullptr);

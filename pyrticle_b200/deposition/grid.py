@@ -17,6 +17,8 @@ from __future__ import annotations
 
 import ctypes as C
 
+import os
+
 import numpy as np
 import torch
 
@@ -175,7 +177,8 @@ def find_points_in_elements(mesh, bricks, el_tolerance, chunk=20000):
         hi_i = np.ceil((ihi_box - brk.origin) / brk.stepwidths).astype(np.int64)
         ext = np.where(nonempty[:, None], np.maximum(hi_i - lo_i, 0), 0)
         mx = ext.max(axis=0)
-        for c0 in range(0, E, chunk):
+
+        def chunk_points(c0):
             sl = slice(c0, min(E, c0 + chunk))
             ee = np.arange(sl.start, sl.stop)
             ox, oy, oz = np.meshgrid(np.arange(mx[0]), np.arange(mx[1]), np.arange(mx[2]),
@@ -195,10 +198,16 @@ def find_points_in_elements(mesh, bricks, el_tolerance, chunk=20000):
             inside = valid & np.all(dist <= scaled_tol[sl][:, None, None], axis=2)
             e_i, k_i = np.nonzero(inside)                                   # row-major
             gidx = brk.start_index + idx[e_i, k_i] @ brk.strides
-            all_el.append(ee[e_i])
-            all_idx.append(gidx)
-            all_pts.append(pts[e_i, k_i])
-            all_w.append(np.full(len(e_i), np.sqrt(dV)))
+            return ee[e_i], gidx, pts[e_i, k_i], np.full(len(e_i), np.sqrt(dV))
+
+        # the element chunks on all host cores, collected in chunk order
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+            for a_el, a_idx, a_pts, a_w in ex.map(chunk_points, range(0, E, chunk)):
+                all_el.append(a_el)
+                all_idx.append(a_idx)
+                all_pts.append(a_pts)
+                all_w.append(a_w)
     el = np.concatenate(all_el)
     order = np.argsort(el, kind="stable")   # bricks in order, points in iterator order
     el = el[order]
@@ -229,7 +238,9 @@ def basis_reduction_matrices(mesh, order, starts, pts, w, max_condition=10.0):
     mats = [None] * E
     kept = np.zeros(E, dtype=np.int64)
     eps = np.finfo(float).eps
-    for P in np.unique(counts):
+
+    def reduce_group(P):
+        """The elements with P points: basis reduction and pseudoinverse."""
         els = np.nonzero(counts == P)[0]
         if P == 0:
             raise RuntimeError("grid depositor: element %d contains no grid points" % els[0])
@@ -276,6 +287,15 @@ def basis_reduction_matrices(mesh, order, starts, pts, w, max_condition=10.0):
             mask[ra, kill_col] = False
             active = ra
             B -= 1
+
+    # the groups are independent: all host cores (LAPACK releases the
+    # interpreter lock; each group's results do not depend on the others)
+    from concurrent.futures import ThreadPoolExecutor
+    sizes = np.unique(counts)
+    order = sorted(sizes, key=lambda P: -int(np.count_nonzero(counts == P)) * int(P))
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        for _ in ex.map(reduce_group, order):
+            pass
     mstarts = np.zeros(E + 1, dtype=np.int64)
     mstarts[1:] = np.cumsum(counts * Np)
     return np.concatenate(mats), mstarts, kept
@@ -295,8 +315,16 @@ def _batched_svd(A):
                 np.stack([o[2] for o in outs]))
 
 
-def orthonormal_vandermonde_fast(points, modes):
-    return refelement.orthonormal_vandermonde(points, modes)
+def orthonormal_vandermonde_fast(points, modes, block=262144):
+    """refelement.orthonormal_vandermonde in blocks of points on all host
+    cores (row by row the same values)."""
+    if len(points) <= block:
+        return refelement.orthonormal_vandermonde(points, modes)
+    from concurrent.futures import ThreadPoolExecutor
+    parts = [points[i:i + block] for i in range(0, len(points), block)]
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        return np.concatenate(list(ex.map(
+            lambda p: refelement.orthonormal_vandermonde(p, modes), parts)))
 
 
 def average_groups(mesh, nodes, nodes_per_element, chunk=None):
