@@ -412,6 +412,15 @@ int prt_remap_grid_to_mesh(const prt_grid *grid, const double *from,
                            double *to, int64_t offset, int64_t increment,
                            void *stream);
 
+/* The remap of 1-4 components at once: from [components][grid nodes] to
+ * [components][DG nodes] (added into `to`, like prt_remap_grid_to_mesh per
+ * component), each element's matrix read once for all components. Same
+ * values as `components` calls of prt_remap_grid_to_mesh. No reference
+ * counterpart (the reference remaps one component per call). */
+int prt_remap_grid_to_mesh_components(const prt_grid *grid, const double *from,
+                                      double *to, int32_t components,
+                                      void *stream);
+
 /* ------------------------------------------------- adjoint (reverse mode) ---
  * No reference counterpart: the reference computes no derivatives. These
  * differentiate prt_lsrk_stage, prt_get_velocities and prt_deposit_shape

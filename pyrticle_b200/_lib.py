@@ -163,6 +163,7 @@ SIGNATURES = {
     "prt_deposit_grid": (_i32, [_vp, _vp, _i32, ShapeFunctionDesc, _i64, _vp, _vp, _vp,
                                 _vp, _vp, _vp, _vp]),
     "prt_remap_grid_to_mesh": (_i32, [_vp, _vp, _vp, _i64, _i64, _vp]),
+    "prt_remap_grid_to_mesh_components": (_i32, [_vp, _vp, _vp, _i32, _vp]),
     "prt_sort_by_element": (_i32, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "prt_lsrk_stage_record": (_i32, [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                      _vp, _vp, _vp, C.POINTER(_vp), _d, _d, _d, _d, _vp]),

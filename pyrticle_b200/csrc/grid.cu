@@ -579,14 +579,19 @@ extern "C" int prt_deposit_grid(const prt_grid *g, prt_workspace *ws, int32_t we
 }
 
 // Remap (dep_grid.hpp:270-358): one warp per element-on-grid; lanes own the
-// element's nodes, the weighted grid values are staged in shared memory.
+// element's nodes, the weighted grid values of NC components are staged in
+// shared memory, and each matrix entry is read once for all components. A
+// block of grid values that is zero in every component is skipped before the
+// matrix is read (fma(M, 0, acc) = acc: the sums are unchanged).
+template <int NC>
 __global__ void remap_kernel(long long eog_count, int np, const uint32_t *__restrict__ els,
                              const uint64_t *__restrict__ starts,
                              const uint32_t *__restrict__ gnodes,
                              const double *__restrict__ weights,
                              const uint64_t *__restrict__ mstarts,
                              const double *__restrict__ mats, const double *__restrict__ from,
-                             double *__restrict__ to, long long offset, long long inc) {
+                             long long from_stride, double *__restrict__ to,
+                             long long to_stride, long long offset, long long inc) {
   extern __shared__ double gv_all[];
   const int warps = blockDim.x >> 5;
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -595,32 +600,54 @@ __global__ void remap_kernel(long long eog_count, int np, const uint32_t *__rest
   const uint64_t s = starts[e];
   const int cnt = (int)(starts[e + 1] - s);
   // stage at most 256 points per pass
-  double *gv = gv_all + wid * 256;
-  double acc[2] = {0, 0};
-  bool any = false;
+  double *gv = gv_all + (size_t)wid * 256 * NC;
+  double acc[NC][2];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) acc[c][0] = acc[c][1] = 0;
+  bool any_total = false;
   const double *M = mats + mstarts[e];
   for (int base = 0; base < cnt; base += 256) {
     const int m = min(256, cnt - base);
+    bool any = false;
     for (int k = lane; k < m; k += 32) {
-      double w = weights[s + base + k] * from[offset + (long long)gnodes[s + base + k] * inc];
-      gv[k] = w;
-      any = any || w != 0;
+      const double wt = weights[s + base + k];
+      const long long gi = offset + (long long)gnodes[s + base + k] * inc;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const double w = wt * from[c * from_stride + gi];
+        gv[c * 256 + k] = w;
+        any = any || w != 0;
+      }
     }
     __syncwarp();
-    for (int k = 0; k < m; ++k) {
-      const double g = gv[k];
-      for (int r = 0; r < 2; ++r) {
-        int i = lane + 32 * r;
-        if (i < np) acc[r] = fma(M[i + (size_t)np * (base + k)], g, acc[r]);
+    if (__any_sync(0xffffffffu, any)) {
+      any_total = true;
+      for (int k = 0; k < m; ++k) {
+        double g[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) g[c] = gv[c * 256 + k];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const int i = lane + 32 * r;
+          if (i < np) {
+            const double Mv = M[i + (size_t)np * (base + k)];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) acc[c][r] = fma(Mv, g[c], acc[c][r]);
+          }
+        }
       }
     }
     __syncwarp();
   }
-  if (!__any_sync(0xffffffffu, any)) return;
-  double *y = to + (long long)els[e] * np * inc + offset;
-  for (int r = 0; r < 2; ++r) {
-    int i = lane + 32 * r;
-    if (i < np) y[i * inc] += acc[r];
+  if (!any_total) return;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    double *y = to + c * to_stride + (long long)els[e] * np * inc + offset;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int i = lane + 32 * r;
+      if (i < np) y[i * inc] += acc[c][r];
+    }
   }
 }
 
@@ -637,22 +664,43 @@ __global__ void average_kernel(long long groups, const uint32_t *__restrict__ st
   for (uint32_t k = s; k < t; ++k) to[offset + (long long)nodes[k] * inc] = avg;
 }
 
+template <int NC>
+int launch_remap(const prt_grid *g, const double *from, long long from_stride, double *to,
+                 long long to_stride, long long offset, long long inc, cudaStream_t s) {
+  if (g->eog_count > 0) {
+    const int warps = 4;
+    remap_kernel<NC><<<prt_grid_blocks(g->eog_count, warps), 32 * warps,
+                       warps * 256 * NC * sizeof(double), s>>>(
+        g->eog_count, g->np, g->eog_elements, g->eog_starts, g->eog_nodes, g->eog_weights,
+        g->eog_mstarts, g->eog_matrices, from, from_stride, to, to_stride, offset, inc);
+    PRT_CHECK_CUDA(cudaGetLastError());
+  }
+  if (g->avg_count > 0)
+    for (int c = 0; c < NC; ++c) {
+      average_kernel<<<prt_grid_blocks(g->avg_count, 128), 128, 0, s>>>(
+          g->avg_count, g->avg_starts, g->avg_nodes, to + c * to_stride, offset, inc);
+      PRT_CHECK_CUDA(cudaGetLastError());
+    }
+  return PRT_OK;
+}
+
 extern "C" int prt_remap_grid_to_mesh(const prt_grid *g, const double *from, double *to,
                                       int64_t offset, int64_t inc, void *stream) {
   if (!g || !from || !to || inc <= 0 || offset < 0 || g->np > 64) return PRT_ERR_INVALID_ARGUMENT;
+  return launch_remap<1>(g, from, 0, to, 0, offset, inc, (cudaStream_t)stream);
+}
+
+extern "C" int prt_remap_grid_to_mesh_components(const prt_grid *g, const double *from,
+                                                 double *to, int32_t components,
+                                                 void *stream) {
+  if (!g || !from || !to || components < 1 || components > 4 || g->np > 64)
+    return PRT_ERR_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;
-  if (g->eog_count > 0) {
-    const int warps = 4;
-    remap_kernel<<<prt_grid_blocks(g->eog_count, warps), 32 * warps,
-                   warps * 256 * sizeof(double), s>>>(
-        g->eog_count, g->np, g->eog_elements, g->eog_starts, g->eog_nodes, g->eog_weights,
-        g->eog_mstarts, g->eog_matrices, from, to, offset, inc);
-    PRT_CHECK_CUDA(cudaGetLastError());
+  const long long G = g->grid_nodes, N = g->mesh->dev.E * (long long)g->np;
+  switch (components) {
+    case 1: return launch_remap<1>(g, from, G, to, N, 0, 1, s);
+    case 2: return launch_remap<2>(g, from, G, to, N, 0, 1, s);
+    case 3: return launch_remap<3>(g, from, G, to, N, 0, 1, s);
+    default: return launch_remap<4>(g, from, G, to, N, 0, 1, s);
   }
-  if (g->avg_count > 0) {
-    average_kernel<<<prt_grid_blocks(g->avg_count, 128), 128, 0, s>>>(
-        g->avg_count, g->avg_starts, g->avg_nodes, to, offset, inc);
-    PRT_CHECK_CUDA(cudaGetLastError());
-  }
-  return PRT_OK;
 }

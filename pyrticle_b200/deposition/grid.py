@@ -507,14 +507,19 @@ class GridDepositor(Depositor):
                                                        out.data_ptr(), 0, 1, self._stream()))
             return out
         out = torch.zeros((q_grid.shape[0], nn), dtype=torch.float64, device=q_grid.device)
-        for c in range(q_grid.shape[0]):
-            _lib.check(self.lib.prt_remap_grid_to_mesh(
-                self.handle, q_grid[c].contiguous().data_ptr(), out[c].data_ptr(), 0, 1,
-                self._stream()))
+        q = q_grid.contiguous()
+        for c0 in range(0, q.shape[0], 4):
+            k = min(4, q.shape[0] - c0)
+            _lib.check(self.lib.prt_remap_grid_to_mesh_components(
+                self.handle, q[c0].data_ptr(), out[c0].data_ptr(), k, self._stream()))
         return out
 
     def deposit_densities_device(self, state, rho=True, j=True):
         gr, gj = self.deposit_grid_densities_device(state, rho, j)
+        if rho and j:
+            # rho and the three j components in one remap pass
+            out = self.remap_grid_to_mesh_device(torch.cat([gr[None], gj]))
+            return out[0], out[1:]
         r = self.remap_grid_to_mesh_device(gr) if rho else None
         jj = self.remap_grid_to_mesh_device(gj) if j else None
         return r, jj

@@ -349,6 +349,26 @@ def test_grid_deposit_and_remap(setup, weights):
         assert gro.sum() * dV == pytest.approx(float(s.charges.sum()), rel=1e-12)
 
 
+def test_grid_remap_components_equal_single_remaps(setup):
+    """The four-component remap (rho and j in one pass) gives bitwise the
+    values of four single-component remaps."""
+    import torch
+    w = setup["w"]
+    m = grid_method(w, "shape")
+    dep = m.depositor
+    s = make_state(m, w)
+    gr, gj = dep.deposit_grid_densities_device(s)
+    q = torch.cat([gr[None], gj]).contiguous()
+    one = torch.zeros((4, len(m.discretization)), dtype=torch.float64, device=q.device)
+    for c in range(4):
+        _lib.check(dep.lib.prt_remap_grid_to_mesh(dep.handle, q[c].data_ptr(), one[c].data_ptr(),
+                                                  0, 1, dep._stream()))
+    four = dep.remap_grid_to_mesh_device(q)
+    assert torch.equal(one, four)
+    rho, j = dep.deposit_densities_device(s)
+    assert torch.equal(rho, one[0]) and torch.equal(j, one[1:])
+
+
 def test_mixed_precision_deposit_error_bounds():
     """The chosen form (tensor-core deposition): rho and j within 1e-5
     relative L2 of the FP64 form (config2's bound), on a
