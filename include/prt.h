@@ -412,6 +412,17 @@ int prt_remap_grid_to_mesh(const prt_grid *grid, const double *from,
                            double *to, int64_t offset, int64_t increment,
                            void *stream);
 
+/* The shape-weight grid deposition of the chosen (mixed) form, on the tensor
+ * cores: the sums of prt_deposit_grid(PRT_GRID_SHAPE) (dep_grid.hpp:220-264)
+ * within ~1e-7 relative, from split-FP16 score MMAs, 23-bit integer weights
+ * and exact int8 MMA sums (the tensor-core form of prt_deposit_shape). Needs
+ * alpha = 2 and bricks numbered contiguously; the grid's points are uploaded
+ * on the first call (24 B per point). Same outputs as prt_deposit_grid. */
+int prt_deposit_grid_mixed(const prt_grid *grid, prt_workspace *ws,
+                           prt_shape_function shape, int64_t n, const double *x,
+                           const double *q, const double *v, const uint32_t *el,
+                           double *grid_rho, double *grid_j, void *stream);
+
 /* The remap of 1-4 components at once: from [components][grid nodes] to
  * [components][DG nodes] (added into `to`, like prt_remap_grid_to_mesh per
  * component), each element's matrix read once for all components. Same

@@ -162,6 +162,8 @@ SIGNATURES = {
     "prt_grid_destroy": (_i32, [_vp]),
     "prt_deposit_grid": (_i32, [_vp, _vp, _i32, ShapeFunctionDesc, _i64, _vp, _vp, _vp,
                                 _vp, _vp, _vp, _vp]),
+    "prt_deposit_grid_mixed": (_i32, [_vp, _vp, ShapeFunctionDesc, _i64, _vp, _vp, _vp, _vp,
+                                      _vp, _vp, _vp]),
     "prt_remap_grid_to_mesh": (_i32, [_vp, _vp, _vp, _i64, _i64, _vp]),
     "prt_remap_grid_to_mesh_components": (_i32, [_vp, _vp, _vp, _i32, _vp]),
     "prt_sort_by_element": (_i32, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -848,9 +848,13 @@ int upload_vec(const std::vector<T> &v, const T **dst) {
 
 // ------------------------------------------------------------ position set
 
-int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
+unsigned long long prt_next_target_uid() {
   static std::atomic<unsigned long long> next_uid{1};
-  m->uid = next_uid++;
+  return next_uid++;
+}
+
+int prt_mesh_build_positions(prt_mesh *m, const prt_mesh_desc *d) {
+  m->uid = prt_next_target_uid();
   const long long E = d->element_count;
   const int Np = d->nodes_per_element;
   const long long nn = E * (long long)Np;

@@ -1167,19 +1167,18 @@ void bisect(const double *P, std::vector<uint32_t> &idx, uint32_t b, uint32_t e,
   }
 }
 
-// The tiles of a mesh for a shape radius, kept in the workspace while mesh
-// and radius stay the same: parts of <= 128 positions from recursive
+// The tiles of a target for a shape radius, kept in the workspace while
+// target and radius stay the same: parts of <= 128 positions from recursive
 // bisection, at most two radii wide along every axis (so that a candidate
 // lies within 2 radii of the tile centre along every axis and the score
 // operands stay in FP16 range); inside a tile the rows are bisected again
 // into compact groups of 32 (one per weight warp's rows). With their
 // bounding boxes and the position operands.
-int tc_tiles(const prt_mesh *mesh, prt_workspace *ws, double radius, cudaStream_t s) {
-  if (ws->tc_mesh_uid == mesh->uid && ws->tc_radius == radius && ws->tc_tiles > 0)
+int tc_tiles(const TcTarget &T, prt_workspace *ws, double radius, cudaStream_t s) {
+  if (ws->tc_mesh_uid == T.uid && ws->tc_radius == radius && ws->tc_tiles > 0)
     return PRT_OK;
-  const PositionSet &PS = mesh->positions;
-  const long long npos = PS.count;
-  const double *P = mesh->pos_host.data();
+  const long long npos = T.npos;
+  const double *P = T.pos_host;
   std::vector<uint32_t> rows((size_t)npos), ts;
   for (long long u = 0; u < npos; ++u) rows[u] = (uint32_t)u;
   ts.reserve(npos / 64 + 2);
@@ -1207,7 +1206,7 @@ int tc_tiles(const prt_mesh *mesh, prt_workspace *ws, double radius, cudaStream_
   // ~1.9 times), wider where a tile's segments could exceed MAXSEG: per axis
   // at most (2 hf + 2 a) / w + 4 bin rows, a row in at most three pieces
   // along a periodic x
-  const bool per_x = mesh->dev.pmin[0] != mesh->dev.pmax[0];
+  const bool per_x = T.mesh->dev.pmin[0] != T.mesh->dev.pmax[0];
   double bw = 0.25 * radius;
   for (;;) {
     const double rows = (2 * hf_max + 2 * radius) / bw + 4;
@@ -1227,18 +1226,17 @@ int tc_tiles(const prt_mesh *mesh, prt_workspace *ws, double radius, cudaStream_
                                  cudaMemcpyHostToDevice, s));
   tile_operands_kernel<<<(unsigned)nt, 128, 0, s>>>(
       nt, (const uint32_t *)set, (const uint32_t *)(set + b_ts + b_tb),
-      (const double *)(set + b_ts), PS.pos, 1.0 / radius, ops);
+      (const double *)(set + b_ts), T.pos, 1.0 / radius, ops);
   PRT_CHECK_CUDA(cudaGetLastError());
   PRT_CHECK_CUDA(cudaStreamSynchronize(s));
-  ws->tc_mesh_uid = mesh->uid;
+  ws->tc_mesh_uid = T.uid;
   ws->tc_radius = radius;
   ws->tc_tiles = nt;
   ws->tc_bin_width = bw;
   return PRT_OK;
 }
 
-int tc_buffers(const prt_mesh *mesh, prt_workspace *ws, long long n, TcPtrs &B) {
-  const PositionSet &PS = mesh->positions;
+int tc_buffers(const TcTarget &T, prt_workspace *ws, long long n, TcPtrs &B) {
   const long long tiles = ws->tc_tiles;
   int rc;
   const size_t b_u64 = align256(8 * (size_t)n), b_u32 = align256(4 * (size_t)n);
@@ -1264,12 +1262,12 @@ int tc_buffers(const prt_mesh *mesh, prt_workspace *ws, long long n, TcPtrs &B) 
   B.tile_ops = (uint4 *)ws_buffer(ws, PRT_WS_TC_TILES, 4096 * (size_t)tiles, &rc);
   if (!B.tile_ops) return rc;
   const size_t b_ts = align256(4 * (size_t)(tiles + 1)), b_tb = align256(48 * (size_t)tiles);
-  char *set = (char *)ws_buffer(ws, PRT_WS_TC_TILESET, b_ts + b_tb + 4 * (size_t)PS.count, &rc);
+  char *set = (char *)ws_buffer(ws, PRT_WS_TC_TILESET, b_ts + b_tb + 4 * (size_t)T.npos, &rc);
   if (!set) return rc;
   B.tile_starts = (const uint32_t *)set;
   B.tile_boxes = (const double *)(set + b_ts);
   B.tile_rows = (const uint32_t *)(set + b_ts + b_tb);
-  B.vals = (double *)ws_buffer(ws, PRT_WS_DEP_VALUES, 4 * sizeof(double) * PS.count, &rc);
+  B.vals = (double *)ws_buffer(ws, PRT_WS_DEP_VALUES, 4 * sizeof(double) * T.npos, &rc);
   if (!B.vals) return rc;
   B.perm = (const uint32_t *)ws_buffer(ws, PRT_WS_DEP_VALS, 8 * (size_t)n, &rc);
   if (!B.perm) return rc;
@@ -1279,10 +1277,10 @@ int tc_buffers(const prt_mesh *mesh, prt_workspace *ws, long long n, TcPtrs &B) 
 
 // The particle bins of the tensor-core deposition (after tc_tiles): the
 // width the tiles chose.
-int tc_bins(const prt_mesh *mesh, const prt_workspace *ws, prt_shape_function shape,
+int tc_bins(const TcTarget &T, const prt_workspace *ws, prt_shape_function shape,
             BinGrid &G) {
   int rc;
-  if (!choose_bins(mesh, mesh->box_lo, mesh->box_hi, ws->tc_bin_width, shape.radius, G, &rc))
+  if (!choose_bins(T.mesh, T.lo, T.hi, ws->tc_bin_width, shape.radius, G, &rc))
     return rc;
   return PRT_OK;
 }
@@ -1291,9 +1289,8 @@ double tc_kappa(prt_shape_function shape) {
   return shape.normalizer * shape.radius * shape.radius / (4.0 * (double)SIGMA * (double)SIGMA);
 }
 
-void tc_args(const prt_mesh *mesh, prt_workspace *ws, prt_shape_function shape,
+void tc_args(const TcTarget &T, prt_workspace *ws, prt_shape_function shape,
              const BinGrid &G, const TcPtrs &B, TcArgs &A) {
-  const PositionSet &PS = mesh->positions;
   A.G = G;
   A.pay = reinterpret_cast<const double2 *>(ws->buf[PRT_WS_DEP_PARTICLES]);
   A.starts = reinterpret_cast<const uint32_t *>(ws->buf[PRT_WS_DEP_BINSTARTS]);
@@ -1313,7 +1310,7 @@ void tc_args(const prt_mesh *mesh, prt_workspace *ws, prt_shape_function shape,
   A.out_scale = B.sc->out;
   A.vals = B.vals;
   A.sums = nullptr;
-  A.npos = PS.count;
+  A.npos = T.npos;
   A.counters = B.counters;
   A.st = ws->status;
 }
@@ -1321,16 +1318,15 @@ void tc_args(const prt_mesh *mesh, prt_workspace *ws, prt_shape_function shape,
 // Steps 1-2 of a call: tile operands, particles binned and packed, the
 // tiles' launch order, the normalising pass (normalising mode), the
 // deposited charge c and c v per particle and their maxima (B.mbits[0..3]).
-int tc_charges(const prt_mesh *mesh, prt_workspace *ws, int32_t mode, prt_shape_function shape,
+int tc_charges(const TcTarget &T, prt_workspace *ws, int32_t mode, prt_shape_function shape,
                const double *iw, long long n, const double *x, const double *q, const double *v,
                const uint32_t *el, bool want_hits, cudaStream_t s, TcPtrs &B, BinGrid &G) {
-  const PositionSet &PS = mesh->positions;
   const bool norm = mode == PRT_DEPOSIT_NORMALIZED;
   int rc;
-  if ((rc = tc_tiles(mesh, ws, shape.radius, s))) return rc;
-  if ((rc = tc_bins(mesh, ws, shape, G))) return rc;
+  if ((rc = tc_tiles(T, ws, shape.radius, s))) return rc;
+  if ((rc = tc_bins(T, ws, shape, G))) return rc;
   const long long tiles = ws->tc_tiles;
-  if ((rc = tc_buffers(mesh, ws, n, B))) return rc;
+  if ((rc = tc_buffers(T, ws, n, B))) return rc;
   const double kappa = tc_kappa(shape);
   // particles binned, sorted and packed (payload weight q, q v)
   DepParticles P;
@@ -1339,23 +1335,23 @@ int tc_charges(const prt_mesh *mesh, prt_workspace *ws, int32_t mode, prt_shape_
     if ((rc = stage_particles(ws, G, n, x, q, v, el, nullptr, 1.0, nullptr, P, s))) return rc;
   }
   // buffers may have moved while staging grew the workspace
-  if ((rc = tc_buffers(mesh, ws, n, B))) return rc;
+  if ((rc = tc_buffers(T, ws, n, B))) return rc;
   candidate_positions_kernel<<<prt_grid_blocks(n, 256), 256, 0, s>>>(n, B.perm, x, G, B.cpos);
   PRT_CHECK_CUDA(cudaGetLastError());
   PRT_CHECK_CUDA(cudaMemsetAsync(B.mbits, 0, 256, s));
   TcArgs A;
-  tc_args(mesh, ws, shape, G, B, A);
+  tc_args(T, ws, shape, G, B, A);
   const unsigned pblocks = (unsigned)((n + 255) / 256);
   const uint32_t *n_live = P.starts + G.nbins;
   if (norm) {
     // position weights -> digits; the normalisation pass
     char *wbuf = (char *)ws_buffer(ws, PRT_WS_TC_WDIG,
-                                   2048 * (size_t)tiles + align256(8 * (size_t)PS.count), &rc);
+                                   2048 * (size_t)tiles + align256(8 * (size_t)T.npos), &rc);
     if (!wbuf) return rc;
     uint4 *wdig = (uint4 *)wbuf;
     double *W = (double *)(wbuf + 2048 * (size_t)tiles);
-    if ((rc = prt_dep_position_weights(mesh, ws, iw, W, s))) return rc;
-    max_abs_kernel<<<592, 256, 0, s>>>(PS.count, W, B.mbits + 4);
+    if ((rc = prt_dep_position_weights(T.mesh, ws, iw, W, s))) return rc;
+    max_abs_kernel<<<592, 256, 0, s>>>(T.npos, W, B.mbits + 4);
     PRT_CHECK_CUDA(cudaGetLastError());
     weight_scale_kernel<<<1, 1, 0, s>>>(B.mbits, kappa, B.sc);
     PRT_CHECK_CUDA(cudaGetLastError());
@@ -1386,10 +1382,10 @@ int tc_charges(const prt_mesh *mesh, prt_workspace *ws, int32_t mode, prt_shape_
 
 // Step 3: charge digits from the maxima (device, [4] doubles), the
 // deposition pass into vals (sums == NULL) or into digit sums.
-int tc_deposit(const prt_mesh *mesh, prt_workspace *ws, prt_shape_function shape, long long n,
+int tc_deposit(const TcTarget &T, prt_workspace *ws, prt_shape_function shape, long long n,
                const BinGrid &G, TcPtrs &B, const double *maxima, double *sums, cudaStream_t s) {
   TcArgs A;
-  tc_args(mesh, ws, shape, G, B, A);
+  tc_args(T, ws, shape, G, B, A);
   A.sums = sums;
   charge_scale_kernel<<<1, 1, 0, s>>>(reinterpret_cast<const unsigned long long *>(maxima),
                                       tc_kappa(shape), B.sc);
@@ -1413,7 +1409,42 @@ int tc_stats(prt_workspace *ws, bool norm, long long n, const TcPtrs &B,
   return PRT_OK;
 }
 
+// A mesh's distinct node positions as a target.
+TcTarget mesh_target(const prt_mesh *mesh) {
+  TcTarget T;
+  T.mesh = mesh;
+  T.uid = mesh->uid;
+  T.npos = mesh->positions.count;
+  T.pos = mesh->positions.pos;
+  T.pos_host = mesh->pos_host.data();
+  for (int a = 0; a < 3; ++a) {
+    T.lo[a] = mesh->box_lo[a];
+    T.hi[a] = mesh->box_hi[a];
+  }
+  return T;
+}
+
 }  // namespace
+
+int prt_deposit_points_tc(const TcTarget &T, prt_workspace *ws, prt_shape_function shape,
+                          long long n, const double *x, const double *q, const double *v,
+                          const uint32_t *el, double *rho, double *j, cudaStream_t s) {
+  TcPtrs B;
+  BinGrid G;
+  int rc;
+  if ((rc = tc_charges(T, ws, PRT_DEPOSIT_PLAIN, shape, nullptr, n, x, q, v, el, false, s, B, G)))
+    return rc;
+  if ((rc = tc_deposit(T, ws, shape, n, G, B, reinterpret_cast<const double *>(B.mbits), nullptr,
+                       s)))
+    return rc;
+  if (rho)
+    PRT_CHECK_CUDA(cudaMemcpyAsync(rho, B.vals, sizeof(double) * T.npos,
+                                   cudaMemcpyDeviceToDevice, s));
+  if (j)
+    PRT_CHECK_CUDA(cudaMemcpyAsync(j, B.vals + T.npos, 3 * sizeof(double) * T.npos,
+                                   cudaMemcpyDeviceToDevice, s));
+  return PRT_OK;
+}
 
 int prt_deposit_shape_tc(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
                          prt_shape_function shape, const double *iw, long long n,
@@ -1423,9 +1454,10 @@ int prt_deposit_shape_tc(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
   TcPtrs B;
   BinGrid G;
   int rc;
-  if ((rc = tc_charges(mesh, ws, mode, shape, iw, n, x, q, v, el, stats != nullptr, s, B, G)))
+  const TcTarget T = mesh_target(mesh);
+  if ((rc = tc_charges(T, ws, mode, shape, iw, n, x, q, v, el, stats != nullptr, s, B, G)))
     return rc;
-  if ((rc = tc_deposit(mesh, ws, shape, n, G, B, reinterpret_cast<const double *>(B.mbits),
+  if ((rc = tc_deposit(T, ws, shape, n, G, B, reinterpret_cast<const double *>(B.mbits),
                        nullptr, s)))
     return rc;
   if ((rc = prt_dep_expand(mesh, B.vals, rho, j, s))) return rc;
@@ -1454,7 +1486,8 @@ extern "C" int prt_deposit_shape_charges(const prt_mesh *mesh, prt_workspace *ws
   TcPtrs B;
   BinGrid G;
   int rc;
-  if ((rc = tc_charges(mesh, ws, mode, shape, iw, n, x, q, v, el, stats != nullptr, s, B, G)))
+  if ((rc = tc_charges(mesh_target(mesh), ws, mode, shape, iw, n, x, q, v, el, stats != nullptr,
+                       s, B, G)))
     return rc;
   PRT_CHECK_CUDA(cudaMemcpyAsync(local_max, B.mbits, 4 * sizeof(double),
                                  cudaMemcpyDeviceToDevice, s));
@@ -1473,9 +1506,10 @@ extern "C" int prt_deposit_shape_sums(const prt_mesh *mesh, prt_workspace *ws,
   TcPtrs B;
   BinGrid G;
   int rc;
-  if ((rc = tc_bins(mesh, ws, shape, G))) return rc;
-  if ((rc = tc_buffers(mesh, ws, n, B))) return rc;
-  return tc_deposit(mesh, ws, shape, n, G, B, global_max, sums, s);
+  const TcTarget T = mesh_target(mesh);
+  if ((rc = tc_bins(T, ws, shape, G))) return rc;
+  if ((rc = tc_buffers(T, ws, n, B))) return rc;
+  return tc_deposit(T, ws, shape, n, G, B, global_max, sums, s);
 }
 
 extern "C" int prt_deposit_shape_combine(const prt_mesh *mesh, prt_workspace *ws,

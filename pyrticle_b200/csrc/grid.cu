@@ -358,6 +358,13 @@ struct prt_grid {
   long long avg_count = 0;
   uint32_t *avg_starts = nullptr;
   uint32_t *avg_nodes = nullptr;
+  // host copy of the jiggled point origins [bricks][3][3] (or empty)
+  std::vector<double> host_origins;
+  // the grid's points in grid-node order, for the tensor-core deposition
+  // (made on its first call)
+  mutable unsigned long long uid = 0;
+  mutable std::vector<double> pt_host;
+  mutable double *pt_dev = nullptr;
 };
 
 extern "C" int prt_grid_create(const prt_mesh *mesh, const prt_grid_desc *d, prt_grid **out) {
@@ -396,6 +403,7 @@ extern "C" int prt_grid_create(const prt_mesh *mesh, const prt_grid_desc *d, prt
   int rc = up(&g->bricks, d->bricks, d->brick_count);
   if (!rc) rc = up(&g->tile_starts, ts.data(), ts.size());
   if (!rc && d->point_origins) {
+    g->host_origins.assign(d->point_origins, d->point_origins + 9 * d->brick_count);
     std::vector<JiggleDev> jg(d->brick_count);
     for (int b = 0; b < d->brick_count && !rc; ++b) {
       const prt_brick &B = d->bricks[b];
@@ -452,8 +460,9 @@ extern "C" int prt_grid_create(const prt_mesh *mesh, const prt_grid_desc *d, prt
 
 extern "C" int prt_grid_destroy(prt_grid *g) {
   if (!g) return PRT_OK;
-  void *ptrs[] = {g->bricks, g->tile_starts, g->jiggle, g->eog_elements, g->eog_starts, g->eog_nodes,
-                  g->eog_weights, g->eog_mstarts, g->eog_matrices, g->avg_starts, g->avg_nodes};
+  void *ptrs[] = {g->bricks,      g->tile_starts, g->jiggle,      g->eog_elements,
+                  g->eog_starts,  g->eog_nodes,   g->eog_weights, g->eog_mstarts,
+                  g->eog_matrices, g->avg_starts, g->avg_nodes,   g->pt_dev};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete g;
@@ -576,6 +585,81 @@ extern "C" int prt_deposit_grid(const prt_grid *g, prt_workspace *ws, int32_t we
         T, G, P, S, grid_rho, grid_j, G_n, g->bricks, nullptr);
   PRT_CHECK_CUDA(cudaGetLastError());
   return PRT_OK;
+}
+
+// The grid's points in grid-node order (host and device), made once: the
+// positions of BrickTarget::point (regular cell centres, or the jiggled
+// points of jiggly_brick::point, grid.hpp:386-396). The bricks must number
+// their points contiguously (brick b starts where brick b-1 ends).
+int grid_points(const prt_grid *g) {
+  if (g->pt_dev) return PRT_OK;
+  long long next = 0;
+  for (const prt_brick &B : g->host_bricks) {
+    if (B.start_index != next) return PRT_ERR_INVALID_ARGUMENT;
+    next += (long long)B.dims[0] * B.dims[1] * B.dims[2];
+  }
+  if (next != g->grid_nodes) return PRT_ERR_INVALID_ARGUMENT;
+  std::vector<double> P(3 * (size_t)g->grid_nodes);
+  for (int b = 0; b < g->brick_count; ++b) {
+    const prt_brick &B = g->host_bricks[b];
+    for (int k = 0; k < B.dims[2]; ++k)
+      for (int jy = 0; jy < B.dims[1]; ++jy)
+        for (int i = 0; i < B.dims[0]; ++i) {
+          const int idx[3] = {i, jy, k};
+          double *p = &P[3 * (size_t)(B.start_index + i +
+                                      (long long)B.dims[0] * (jy + (long long)B.dims[1] * k))];
+          for (int a = 0; a < 3; ++a)
+            p[a] = g->host_origins.empty()
+                       ? B.origin[a] + B.stepwidths[a] / 2 + idx[a] * B.stepwidths[a]
+                       : g->host_origins[9 * b + 3 * ((i + jy + k) % 3) + a] +
+                             idx[a] * B.stepwidths[a];
+        }
+  }
+  double *d = nullptr;
+  PRT_CHECK_CUDA(cudaMalloc((void **)&d, P.size() * sizeof(double)));
+  if (cudaMemcpy(d, P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return PRT_ERR_CUDA;
+  }
+  g->pt_host.swap(P);
+  g->pt_dev = d;
+  g->uid = prt_next_target_uid();
+  return PRT_OK;
+}
+
+extern "C" int prt_deposit_grid_mixed(const prt_grid *g, prt_workspace *ws,
+                                      prt_shape_function shape, int64_t n, const double *x,
+                                      const double *q, const double *v, const uint32_t *el,
+                                      double *grid_rho, double *grid_j, void *stream) {
+  if (!g || !ws || n < 0 || n >= (1ll << 31)) return PRT_ERR_INVALID_ARGUMENT;
+  if (shape.alpha != 2 || !(shape.radius > 0)) return PRT_ERR_INVALID_ARGUMENT;
+  if (n > 0 && (!x || !q || (grid_j && !v))) return PRT_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc;
+  if ((rc = grid_points(g))) return rc;
+  const long long G_n = g->grid_nodes;
+  if (n == 0) {
+    if (grid_rho) PRT_CHECK_CUDA(cudaMemsetAsync(grid_rho, 0, G_n * sizeof(double), s));
+    if (grid_j) PRT_CHECK_CUDA(cudaMemsetAsync(grid_j, 0, 3 * G_n * sizeof(double), s));
+    return PRT_OK;
+  }
+  TcTarget T;
+  T.mesh = g->mesh;
+  T.uid = g->uid;
+  T.npos = G_n;
+  T.pos = g->pt_dev;
+  T.pos_host = g->pt_host.data();
+  // particle bins over the mesh box and the bricks
+  for (int d = 0; d < 3; ++d) {
+    T.lo[d] = g->mesh->box_lo[d];
+    T.hi[d] = g->mesh->box_hi[d];
+  }
+  for (const prt_brick &B : g->host_bricks)
+    for (int d = 0; d < 3; ++d) {
+      T.lo[d] = std::min(T.lo[d], B.origin[d]);
+      T.hi[d] = std::max(T.hi[d], B.origin[d] + B.dims[d] * B.stepwidths[d]);
+    }
+  return prt_deposit_points_tc(T, ws, shape, n, x, q, v, el, grid_rho, grid_j, s);
 }
 
 // Remap (dep_grid.hpp:270-358): one warp per element-on-grid; lanes own the

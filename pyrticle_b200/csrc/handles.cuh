@@ -160,3 +160,22 @@ int prt_deposit_shape_tc(const prt_mesh *mesh, prt_workspace *ws, int32_t mode,
                          const double *x, const double *q, const double *v,
                          const uint32_t *el, double *rho, double *j,
                          prt_deposit_stats *stats, cudaStream_t s);
+
+// A unique id per mesh or grid (the workspace caches key on it).
+unsigned long long prt_next_target_uid();
+
+// The points a tensor-core deposition sums onto: a mesh's distinct node
+// positions or a grid's brick points.
+struct TcTarget {
+  const prt_mesh *mesh = nullptr;  // periodicity
+  unsigned long long uid = 0;
+  long long npos = 0;
+  const double *pos = nullptr;       // device [npos][3]
+  const double *pos_host = nullptr;  // host [npos][3]
+  double lo[3], hi[3];               // box the particle bins cover
+};
+// The plain shape deposition (alpha = 2) onto a target's points on the tensor
+// cores: rho [npos] and j [3][npos] (either may be NULL).
+int prt_deposit_points_tc(const TcTarget &T, prt_workspace *ws, prt_shape_function shape,
+                          long long n, const double *x, const double *q, const double *v,
+                          const uint32_t *el, double *rho, double *j, cudaStream_t s);

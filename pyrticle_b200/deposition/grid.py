@@ -383,13 +383,23 @@ def average_groups(mesh, nodes, nodes_per_element, chunk=None):
 
 class GridDepositor(Depositor):
     """Deposit on brick grids (shape-function values at the points, or
-    trilinear weights with ``grid_weights="trilinear"``), then remap."""
+    trilinear weights with ``grid_weights="trilinear"``), then remap.
+
+    ``precision``: ``"fp64"`` (the reference's arithmetic) or ``"mixed"``
+    (the chosen form: the shape-weight grid deposition on the tensor cores,
+    split-FP16 scores, 23-bit integer weights, exact int8 sums; shape
+    weights with exponent 2 only). The remap is FP64 in both."""
+
+    PRECISIONS = ("fp64", "mixed")
 
     def __init__(self, brick_generator=None, el_tolerance=0.12, max_extra_points=20,
                  enforce_continuity=False, submethod="simplex_reduce",
                  filter_min_amplification=None, filter_order=None, jiggle_radius=0.0,
-                 grid_weights="shape"):
+                 grid_weights="shape", precision="fp64"):
         Depositor.__init__(self)
+        if precision not in self.PRECISIONS:
+            raise ValueError(f"precision must be one of {self.PRECISIONS}")
+        self.precision = precision
         self.brick_generator = brick_generator or SingleBrickGenerator()
         self.el_tolerance = el_tolerance
         self.max_extra_points = max_extra_points
@@ -490,6 +500,16 @@ class GridDepositor(Depositor):
         gr = torch.empty((G,), dtype=torch.float64, device=dev) if rho else None
         gj = torch.empty((3, G), dtype=torch.float64, device=dev) if j else None
         v = m.velocities_device(state) if j else None
+        if self.precision == "mixed":
+            if self.grid_weights != "shape" or self.shape_function is None or \
+                    self.shape_function.exponent != 2:
+                raise ValueError("the mixed grid deposition needs shape weights with exponent 2")
+            _lib.check(self.lib.prt_deposit_grid_mixed(
+                self.handle, m.workspace, self._shape_desc(), len(state),
+                state.x.data_ptr(), state.q.data_ptr(), v.data_ptr() if v is not None else None,
+                state.el.data_ptr(), gr.data_ptr() if rho else None,
+                gj.data_ptr() if j else None, self._stream()), "prt_deposit_grid_mixed")
+            return gr, gj
         wmode = _lib.GRID_SHAPE if self.grid_weights == "shape" else _lib.GRID_TRILINEAR
         _lib.check(self.lib.prt_deposit_grid(
             self.handle, m.workspace, wmode, self._shape_desc(), len(state),

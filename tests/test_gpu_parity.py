@@ -349,6 +349,30 @@ def test_grid_deposit_and_remap(setup, weights):
         assert gro.sum() * dV == pytest.approx(float(s.charges.sum()), rel=1e-12)
 
 
+@pytest.mark.parametrize("jiggle", [0.0, 0.3])
+def test_grid_mixed_matches_fp64(setup, jiggle):
+    """The chosen-form grid deposition (tensor cores) against the FP64 grid
+    deposition: rho and j within 1e-5 relative L2 (the chosen form's bound;
+    ~1e-7 expected), bitwise repeatable, and the same remapped values'
+    relation."""
+    import torch
+    w = setup["w"]
+    gen = SingleBrickGenerator(dims=(24, 24, 96))
+    out = {}
+    for prec in ("fp64", "mixed"):
+        dep = GridDepositor(brick_generator=gen, jiggle_radius=jiggle, precision=prec)
+        m = make_method(w, depositor=dep)
+        m.depositor.set_shape_function(None, PolynomialShapeFunction(w.shape_radius, 3, 2))
+        s = make_state(m, w)
+        out[prec] = dep.deposit_grid_densities_device(s)
+        if prec == "mixed":
+            again = dep.deposit_grid_densities_device(s)
+            assert torch.equal(out[prec][0], again[0]) and torch.equal(out[prec][1], again[1])
+    (r64, j64), (r32, j32) = out["fp64"], out["mixed"]
+    assert float(torch.linalg.norm(r32 - r64) / torch.linalg.norm(r64)) < 1e-5
+    assert float(torch.linalg.norm(j32 - j64) / torch.linalg.norm(j64)) < 1e-5
+
+
 def test_grid_remap_components_equal_single_remaps(setup):
     """The four-component remap (rho and j in one pass) gives bitwise the
     values of four single-component remaps."""
