@@ -23,13 +23,16 @@
 //     coordinates (v = 2 SIGMA w), the position term SIGMA (1 - |u|^2) and
 //     the particle term -SIGMA |w|^2, each as two terms; the tensor cores
 //     accumulate in FP32 into tensor memory;
-//  3. weight: each thread reads its position's row (tcgen05.ld), forms
+//  3. weight: each thread reads its row (tcgen05.ld), forms
 //     t = s + |s| = 2 max(s, 0) and the integer F = round(t^2) =
 //     round(4 SIGMA^2 max(1 - r^2/a^2, 0)^2) < 2^23 with one FMA
 //     (t t + 2^23 puts the rounded integer in the low mantissa bits), and
-//     stores its three bytes as unsigned 8-bit digits in shared memory;
-//  4. sums: tcgen05.mma kind::i8 (int32 accumulation in tensor memory,
-//     exact) of the weight digits against
+//     writes the word back in place (tcgen05.st): its bytes 0-2 are F's
+//     base-256 digits, byte 3 a constant;
+//  4. sums: tcgen05.mma kind::i8 with A in tensor memory (the weight words
+//     as unsigned 8-bit K elements; int32 accumulation, exact) against digit
+//     rows in shared memory laid out so that three views one row apart
+//     multiply bytes 2, 1 and 0 by the digits and byte 3 by zero (N = 48):
 //      - deposition: per candidate the charge c (q or q / integral) scaled
 //        to a signed integer below 2^46 in six balanced signed digits and
 //        c v (each component below 2^22, three digits), one 16-column
@@ -39,8 +42,8 @@
 //        could overflow);
 //      - normalisation: per position the weight sum_{nodes} |J_e| w_i (which
 //        is negative at some nodes of order 2 and 4 elements) as a 47-bit
-//        signed integer in six balanced signed digits; the weight digits are read
-//        transposed (MN-major: the same bytes are rows = candidates), so the
+//        signed integer in six balanced signed digits; this pass scores with
+//        rows = candidates (the same products, so bitwise the same F), so the
 //        product is, per candidate, sum_u F W over the tile, which the CTA
 //        adds to the particle's integral as two exact 64-bit integer atomics
 //        (signed high part, low 40 bits): integer sums do not depend on the
@@ -55,9 +58,11 @@
 // Synchronisation per chunk k of a CTA: the score MMA of chunk k and the
 // accumulation MMA of chunk k-1 run while the warps stage chunk k+1 (the
 // ring of five chunks holds chunks k-1 .. k+1 and at most 255 slots more);
-// the weights of chunk k are written once the accumulation MMA of chunk k-1
-// has completed (mbarrier); one thread of a warp that stages nothing issues
-// the score MMA of chunk k+1 and the accumulation MMA of chunk k. Every
+// the weights of chunk k are written over its scores once they are ready
+// (mbarrier); one thread of a warp that stages nothing issues the
+// accumulation MMA of chunk k and then the score MMA of chunk k+1 (the MMAs
+// of one thread run in issue order, so the scores overwrite the weight words
+// only after the accumulation has read them). Every
 // mbarrier wait is bounded: a CTA whose wait runs out records PRT_ERR_TIMEOUT,
 // stops, waits (bounded) for its issued MMAs and frees its tensor memory.
 
@@ -83,8 +88,7 @@ constexpr int FILL_WARPS = 7;    // warps 0-6 stage candidates
 constexpr int ISSUE_WARP = 7;    // warp 7 issues the tensor-core work
 constexpr int MAXSEG = 512;      // bin-row segments per tile
 constexpr uint32_t TMEM_COLS = 256;
-constexpr uint32_t COL_ACC = 128;  // accumulators: weight digit d at +16 d, indicator at +48
-constexpr int FDIG = 3;            // weight digits (bytes 2, 1, 0 of the weight)
+constexpr uint32_t COL_ACC = 128;  // accumulators: weight byte 2 - j at +16 j (j = 0, 1, 2)
 constexpr float SIGMA = 1448.0f;   // 4 SIGMA^2 < 2^23
 constexpr int FLUSH_CHUNKS = 256;    // int32 accumulation window (256 * 128 * 255 * 128 < 2^31)
 constexpr int CDIG = 6, JDIG = 3, WDIG = 6;
@@ -93,13 +97,19 @@ constexpr int CDIG = 6, JDIG = 3, WDIG = 6;
 struct Smem {
   uint8_t apos[2 * TM * 16];     // position operand, K-major: [K chunk][row][16 B]
   uint8_t bcand[2 * RING * 16];  // candidate operands, K-major: [K chunk][slot][16 B]
+  // The sums' B operand (MN-major rows of 16 digit bytes, one row per K): a
+  // weight word holds the K elements 4 c .. 4 c + 3 (bytes 0-3 of F + 2^23),
+  // so each candidate (deposition) or position (normalisation) c has four
+  // rows, its digits in row 4 c + 3 and zeros in 4 c .. 4 c + 2; three views
+  // one row apart (SBO 16 bytes) multiply bytes 2, 1, 0 by the digits
   union {
-    uint8_t bdig[RING * 16];     // deposition: charge digits per slot (16 columns, MN-major)
-    uint32_t slot_id[RING];      // normalisation: bin-order particle of a slot
+    uint8_t zdig[(4 * RING + 3) * 16];  // deposition: charge digits per slot
+    struct {
+      uint8_t zw[(4 * TM + 3) * 16];    // normalisation: position weight digits
+      uint32_t slot_id[RING];           // bin-order particle of a slot
+    } n;
+    double tsum[TM][16];                // deposition epilogue: digit sums per position
   };
-  uint8_t wdig[TM * 16];         // weight digits per position (16 columns, MN-major)
-  // weight digits: [byte 2, byte 1, byte 0, indicator][16-candidate block][position][16 B]
-  uint8_t fdig[FDIG + 1][NC / 16][TM][16];
   // per segment: the origin of its first bin relative to the tile centre
   // (periodic image included) and that bin's x index
   float4 seg_o[MAXSEG];
@@ -159,12 +169,14 @@ __device__ __forceinline__ void mma_f16(uint32_t d, uint64_t a, uint64_t b, uint
       : "memory");
 }
 
-__device__ __forceinline__ void mma_i8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
-                                       uint32_t acc) {
+// int8 MMA with A in tensor memory (K-major: each 32-bit column holds four
+// consecutive K elements), B in shared memory
+__device__ __forceinline__ void mma_i8_ts(uint32_t d, uint32_t a_tmem, uint64_t b, uint32_t idesc,
+                                          uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
-      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d),
+      "r"(a_tmem), "l"(b), "r"(idesc), "r"(acc)
       : "memory");
 }
 
@@ -232,6 +244,24 @@ __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ void tmem_st32(uint32_t addr, const uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, "
+      "%17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};\n" ::"r"(
+          addr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]),
+      "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]),
+      "r"(r[29]), "r"(r[30]), "r"(r[31])
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
 // FP32 -> (high, low) FP16 terms
 __device__ __forceinline__ void split_half(float x, __half &h, __half &l) {
   h = __float2half_rn(x);
@@ -240,12 +270,6 @@ __device__ __forceinline__ void split_half(float x, __half &h, __half &l) {
 
 __device__ __forceinline__ uint32_t pack2(__half a, __half b) {
   return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
-}
-
-__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
-  uint32_t d;
-  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
-  return d;
 }
 
 // The candidate operand of a particle at w (relative to the tile centre, in
@@ -473,9 +497,9 @@ __device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const float hf[3]
       *reinterpret_cast<uint4 *>(S.bcand + (size_t)slot * 16) = k0;
       *reinterpret_cast<uint4 *>(S.bcand + (size_t)(RING + slot) * 16) = k1;
       if (NORM)
-        S.slot_id[slot] = k;
+        S.n.slot_id[slot] = k;
       else
-        *reinterpret_cast<uint4 *>(S.bdig + (size_t)slot * 16) = B.dig;
+        *reinterpret_cast<uint4 *>(S.zdig + (size_t)(4 * slot + 3) * 16) = B.dig;
     }
     next_batch<NORM>(S, A, C, B, lane);
   };
@@ -494,69 +518,53 @@ __device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const float hf[3]
 }
 
 // Zeroes the candidate operands of slots [from, to) of a ring chunk (the
-// tail of the last chunk): a zero operand gives score 0, weight 0.
+// tail of the last chunk): a zero operand gives score 0, weight 0, so the
+// slots' digit rows (stale) are multiplied by zero.
 __device__ __forceinline__ void pad_chunk(Smem &S, int from, int to, int tid) {
   for (int i = from + tid; i < to; i += THREADS) {
     const int slot = i % RING;
     *reinterpret_cast<uint4 *>(S.bcand + (size_t)slot * 16) = make_uint4(0, 0, 0, 0);
     *reinterpret_cast<uint4 *>(S.bcand + (size_t)(RING + slot) * 16) = make_uint4(0, 0, 0, 0);
-    *reinterpret_cast<uint4 *>(S.bdig + (size_t)slot * 16) = make_uint4(0, 0, 0, 0);
   }
 }
 
-// Weight digits of one chunk from its scores in tensor memory: thread
-// (warp w, lane l) takes position row 32 (w % 4) + l and candidate columns
-// 64 (w / 4) .. + 63.
-template <bool IND>
-__device__ __forceinline__ void weights(Smem &S, uint32_t tmem, int warp, int lane) {
-  const int q = warp & 3, h = warp >> 2;
-  const int row = 32 * q + lane;
+// The weights of one chunk, in place in tensor memory: thread (warp w, lane
+// l) takes row 32 (w % 4) + l (a position in the deposition pass, a
+// candidate in the normalisation pass) and columns 64 (w / 4) .. + 63, reads
+// the scores s (tcgen05.ld), and writes back the words F + 2^23 with
+// F = round(t^2), t = s + |s| (one FMA: t t + 2^23 puts the rounded integer
+// in the low mantissa bits), so bytes 0-2 are F's base-256 digits and byte 3
+// a constant the sums multiply by zero. Counts the words with F > 0 (hits).
+template <bool HITS>
+__device__ __forceinline__ uint32_t weights(uint32_t tmem, int warp, int lane) {
+  const uint32_t base = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(64 * (warp >> 2));
+  uint32_t hits = 0;
 #pragma unroll 1
   for (int half = 0; half < 2; ++half) {
     uint32_t r[32];
-    tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(64 * h + 32 * half), r);
+    tmem_ld32(base + 32 * half, r);
     tmem_wait_ld();
 #pragma unroll
-    for (int g = 0; g < 2; ++g) {
-      uint32_t b0[4], b1[4], b2[4], ind[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        uint32_t b[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const float s = __uint_as_float(r[16 * g + 4 * j + e]);
-          const float t = s + fabsf(s);                     // 2 max(s, 0), exact
-          b[e] = __float_as_uint(fmaf(t, t, 8388608.0f));  // 2^23 + round(t^2)
-        }
-        const uint32_t x = prmt(b[0], b[1], 0x5140), y = prmt(b[2], b[3], 0x5140);
-        const uint32_t z = prmt(b[0], b[1], 0x0062), w = prmt(b[2], b[3], 0x0062);
-        b0[j] = prmt(x, y, 0x5410);  // byte 0 of each value
-        b1[j] = prmt(x, y, 0x7632);  // byte 1
-        b2[j] = prmt(z, w, 0x5410);  // byte 2
-        if (IND) ind[j] = __vcmpne4(b0[j] | b1[j] | b2[j], 0u) & 0x01010101u;
-      }
-      const int blk = (64 * h + 32 * half + 16 * g) >> 4;
-      *reinterpret_cast<uint4 *>(&S.fdig[0][blk][row][0]) = make_uint4(b2[0], b2[1], b2[2], b2[3]);
-      *reinterpret_cast<uint4 *>(&S.fdig[1][blk][row][0]) = make_uint4(b1[0], b1[1], b1[2], b1[3]);
-      *reinterpret_cast<uint4 *>(&S.fdig[2][blk][row][0]) = make_uint4(b0[0], b0[1], b0[2], b0[3]);
-      if (IND)
-        *reinterpret_cast<uint4 *>(&S.fdig[FDIG][blk][row][0]) =
-            make_uint4(ind[0], ind[1], ind[2], ind[3]);
+    for (int i = 0; i < 32; ++i) {
+      const float sc = __uint_as_float(r[i]);
+      const float t = sc + fabsf(sc);                        // 2 max(s, 0), exact
+      r[i] = __float_as_uint(fmaf(t, t, 8388608.0f));        // 2^23 + round(t^2)
+      if (HITS) hits += r[i] != 0x4B000000u;
     }
+    tmem_st32(base + 32 * half, r);
   }
+  tmem_wait_st();
+  return hits;
 }
 
 // Instruction descriptors (M = 128):
 //  score: D FP32, A/B FP16, both K-major, N = 128
 constexpr uint32_t IDESC_SCORE =
     (1u << 4) | ((uint32_t)(NC >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
-//  deposition sums: D S32, A U8 K-major (weights, rows = positions), B S8
-//  MN-major (charge digits), N = 16
-constexpr uint32_t IDESC_DEP = (2u << 4) | (1u << 10) | (1u << 16) | (2u << 17) | (8u << 24);
-//  normalisation sums: D S32, A U8 MN-major (weights read as rows =
-//  candidates), B S8 MN-major (position weight digits), N = 16
-constexpr uint32_t IDESC_NORM =
-    (2u << 4) | (1u << 10) | (1u << 15) | (1u << 16) | (2u << 17) | (8u << 24);
+//  sums: D S32, A U8 K-major in tensor memory (the weight words, rows =
+//  positions or candidates), B S8 MN-major (digit rows), N = 48 (three
+//  views of the digit rows: weight bytes 2, 1, 0)
+constexpr uint32_t IDESC_SUMS = (2u << 4) | (1u << 10) | (1u << 16) | (6u << 17) | (8u << 24);
 
 // rho, j of a position from its digit sums T (T_i = sum_p F c_i over the
 // particles, c_i the i-th digit column): charge = sum_i T_i 256^i over the
@@ -611,9 +619,15 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   {
     const uint4 *src = A.tile_ops + (size_t)tile * 256;
     for (int i = tid; i < 256; i += THREADS) reinterpret_cast<uint4 *>(S.apos)[i] = src[i];
+    // the digit rows: zeros, then (normalisation) each position's weight
+    // digits in its row 4 u + 3
+    uint4 *z = reinterpret_cast<uint4 *>(NORM ? S.n.zw : S.zdig);
+    const int zrows = NORM ? 4 * TM + 3 : 4 * RING + 3;
+    for (int i = tid; i < zrows; i += THREADS) z[i] = make_uint4(0, 0, 0, 0);
     if (NORM) {
+      __syncthreads();
       const uint4 *ws = A.wdig + (size_t)tile * 128;
-      for (int i = tid; i < 128; i += THREADS) reinterpret_cast<uint4 *>(S.wdig)[i] = ws[i];
+      for (int i = tid; i < 128; i += THREADS) z[4 * i + 3] = ws[i];
     }
   }
   __syncthreads();
@@ -624,8 +638,15 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   fence_after();
   const uint32_t tmem = S.tmem;
   const uint32_t bar_s = smem_u32(&S.bar_s), bar_a = smem_u32(&S.bar_a);
-  const uint32_t a_pos = smem_u32(S.apos), b_cand = smem_u32(S.bcand), b_dig = smem_u32(S.bdig);
-  const uint32_t w_dig = smem_u32(S.wdig), f_dig = smem_u32(S.fdig);
+  const uint32_t a_pos = smem_u32(S.apos), b_cand = smem_u32(S.bcand);
+  const uint32_t z_dig = smem_u32(NORM ? S.n.zw : S.zdig);
+  // the scores of the chunk at ring slot `slot`: rows = positions
+  // (deposition) or candidates (normalisation), the same products either way
+  auto score_mma = [&](int slot) {
+    const uint64_t dp = sdesc(a_pos, TM * 16, 128);
+    const uint64_t dc = sdesc(b_cand + (uint32_t)(slot * 16), RING * 16, 128);
+    mma_f16(tmem, NORM ? dc : dp, NORM ? dp : dc, IDESC_SCORE, 0);
+  };
 
   // per thread: position row 32 (warp % 4) + lane, digit columns
   // 8 (warp / 4) .. + 7 of the deposition's sums over the weight digits
@@ -647,15 +668,14 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
 
   // readout of a normalisation chunk: per candidate its sum over the tile,
   // P = H 2^40 + L (0 <= L < 2^40), both parts added exactly to the
-  // particle's integral (H modulo 2^64): warps 0-3 add H, warps 4-7 add L and
-  // the hit count (a warp reads the tensor-memory lanes 32 (warp % 4) ..)
+  // particle's integral (H modulo 2^64): warps 0-3 add H, warps 4-7 add L (a
+  // warp reads the tensor-memory lanes 32 (warp % 4) ..)
   auto norm_readout = [&](int chunk, int nvalid) {
-    uint32_t d2[8], d1[8], d0[8], di[8];
+    uint32_t d2[8], d1[8], d0[8];
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
     tmem_ld8(lane_addr + COL_ACC, d2);
     tmem_ld8(lane_addr + COL_ACC + 16, d1);
     tmem_ld8(lane_addr + COL_ACC + 32, d0);
-    if (IND && warp >= 4) tmem_ld8(lane_addr + COL_ACC + 48, di);
     tmem_wait_ld();
     const int cr = 32 * (warp & 3) + lane;
     if (cr < nvalid) {
@@ -671,12 +691,11 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
       const long long l1 = (plo & M40) + ((phi & 0xffff) << 24);  // < 2^41
       const long long L = l1 & M40;
       const long long H = (plo >> 40) + (phi >> 16) + (l1 >> 40);
-      const uint32_t id = S.slot_id[(chunk * NC + cr) % RING];
+      const uint32_t id = S.n.slot_id[(chunk * NC + cr) % RING];
       if (warp < 4) {
         if (H != 0) atomicAdd(A.norm_hi + id, (unsigned long long)H);
       } else {
         if (L != 0) atomicAdd(A.norm_lo + id, (unsigned long long)L);
-        if (IND && di[WDIG]) atomicAdd(A.hits + id, di[WDIG]);
       }
     }
   };
@@ -712,7 +731,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     __syncthreads();
     if (valid > 0 && issuer) {
       fence_after();
-      mma_f16(tmem, sdesc(a_pos, TM * 16, 128), sdesc(b_cand, RING * 16, 128), IDESC_SCORE, 0);
+      score_mma(0);
       mma_commit(bar_s);
     }
     if (valid > 0) ++issued_s;
@@ -747,7 +766,12 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
       if (w) {
         ++waited_s;
         fence_after();
-        weights<NORM && IND>(S, tmem, warp, lane);
+        const uint32_t h = weights<NORM && IND>(tmem, warp, lane);
+        if (NORM && IND && h) {
+          // the hits of this thread's candidate among its 64 positions
+          const int cr = 32 * (warp & 3) + lane;
+          if (cr < valid) atomicAdd(A.hits + S.n.slot_id[(k * NC + cr) % RING], h);
+        }
       }
     }
     fence_async_smem();
@@ -761,36 +785,25 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
       fence_async_smem();
       __syncthreads();
     }
-    // (4) the scores of chunk k+1, then the sums of chunk k (the issue warp;
-    // the fill warps go on to chunk k+2)
+    // (4) the sums of chunk k, then the scores of chunk k+1 (the issue warp;
+    // the fill warps go on to chunk k+2). The sums read chunk k's weight
+    // words from the tensor-memory columns the next scores overwrite: the
+    // MMAs of one thread run in issue order.
     if (issuer) {
       fence_after();
+      const int slot0 = (k * NC) % RING;
+      const uint32_t zb = z_dig + (NORM ? 0u : (uint32_t)(64 * slot0));
+#pragma unroll
+      for (int kk = 0; kk < NC / 8; ++kk)
+        mma_i8_ts(tmem + COL_ACC, tmem + (uint32_t)(8 * kk),
+                  sdesc(zb + (uint32_t)(16 * (32 * kk + 1)), 128, 16), IDESC_SUMS,
+                  (kk > 0 || (!NORM && window > 0)) ? 1u : 0u);
+      mma_commit(bar_a);
       if (valid_next > 0) {
         const int slot1 = ((k + 1) * NC) % RING;
-        mma_f16(tmem, sdesc(a_pos, TM * 16, 128), sdesc(b_cand + slot1 * 16, RING * 16, 128),
-                IDESC_SCORE, 0);
+        score_mma(slot1);
         mma_commit(bar_s);
       }
-      const int slot0 = (k * NC) % RING;
-      if (NORM) {
-#pragma unroll
-        for (int d = 0; d < (IND ? FDIG + 1 : FDIG); ++d)
-#pragma unroll
-          for (int jj = 0; jj < 4; ++jj)
-            mma_i8(tmem + COL_ACC + 16 * d,
-                   sdesc(f_dig + d * (NC / 16) * TM * 16 + jj * 512, 128, (uint32_t)TM * 16),
-                   sdesc(w_dig + jj * 512, 128, 128), IDESC_NORM, jj > 0);
-      } else {
-#pragma unroll
-        for (int d = 0; d < FDIG; ++d)
-#pragma unroll
-          for (int jj = 0; jj < 4; ++jj)
-            mma_i8(tmem + COL_ACC + 16 * d,
-                   sdesc(f_dig + d * (NC / 16) * TM * 16 + jj * 2 * TM * 16, TM * 16, 128),
-                   sdesc(b_dig + (slot0 + 32 * jj) * 16, 128, 128), IDESC_DEP,
-                   (window > 0 || jj > 0) ? 1u : 0u);
-      }
-      mma_commit(bar_a);
     }
     ++issued_a;
     if (valid_next > 0) ++issued_s;
@@ -825,7 +838,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     if (!NORM) {
       // per position the 16 digit sums T_i (exact integers), then the charge
       // (six digits) and current (three digits per component)
-      double(*tsum)[16] = reinterpret_cast<double(*)[16]>(&S.fdig[0][0][0][0]);
+      double(*tsum)[16] = S.tsum;
       const int row = 32 * (warp & 3) + lane;
 #pragma unroll
       for (int i = 0; i < 8; ++i) tsum[row][8 * (warp >> 2) + i] = acc[i];
