@@ -107,6 +107,7 @@ struct Smem {
     struct {
       uint8_t zw[(4 * TM + 3) * 16];    // normalisation: position weight digits
       uint32_t slot_id[RING];           // bin-order particle of a slot
+      uint32_t hits[2][2][NC];          // [chunk parity][column half][candidate]
     } n;
     double tsum[TM][16];                // deposition epilogue: digit sums per position
   };
@@ -668,8 +669,8 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
 
   // readout of a normalisation chunk: per candidate its sum over the tile,
   // P = H 2^40 + L (0 <= L < 2^40), both parts added exactly to the
-  // particle's integral (H modulo 2^64): warps 0-3 add H, warps 4-7 add L (a
-  // warp reads the tensor-memory lanes 32 (warp % 4) ..)
+  // particle's integral (H modulo 2^64): warps 0-3 add H, warps 4-7 add L
+  // and the hit count (a warp reads the tensor-memory lanes 32 (warp % 4) ..)
   auto norm_readout = [&](int chunk, int nvalid) {
     uint32_t d2[8], d1[8], d0[8];
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
@@ -696,6 +697,10 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
         if (H != 0) atomicAdd(A.norm_hi + id, (unsigned long long)H);
       } else {
         if (L != 0) atomicAdd(A.norm_lo + id, (unsigned long long)L);
+        if (IND) {
+          const uint32_t h = S.n.hits[chunk & 1][0][cr] + S.n.hits[chunk & 1][1][cr];
+          if (h) atomicAdd(A.hits + id, h);
+        }
       }
     }
   };
@@ -767,11 +772,9 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
         ++waited_s;
         fence_after();
         const uint32_t h = weights<NORM && IND>(tmem, warp, lane);
-        if (NORM && IND && h) {
-          // the hits of this thread's candidate among its 64 positions
-          const int cr = 32 * (warp & 3) + lane;
-          if (cr < valid) atomicAdd(A.hits + S.n.slot_id[(k * NC + cr) % RING], h);
-        }
+        // the hits of this thread's candidate among its 64 positions, added
+        // to the particle with the readout
+        if (NORM && IND) S.n.hits[k & 1][warp >> 2][32 * (warp & 3) + lane] = h;
       }
     }
     fence_async_smem();
