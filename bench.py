@@ -813,14 +813,17 @@ def main():
         keep = []
         for k in range(args.steps):
             cur, nxt = k % 2, (k + 1) % 2
-            comp.wait_event(up[cur])
-            rho, j = one_step_on(stores[cur])
-            done[cur].record(comp)
-            keep.append((rho, j))
+            # the next step's inputs are enqueued before this step (the
+            # normalising depositor's statistics make each step wait for
+            # itself on the host), into the store the previous step used
             if k + 1 < args.steps:
                 if k >= 1:
                     copy.wait_event(done[nxt])  # the store's previous step is done
                 upload(stores[nxt], nxt)
+            comp.wait_event(up[cur])
+            rho, j = one_step_on(stores[cur])
+            done[cur].record(comp)
+            keep.append((rho, j))
             with torch.cuda.stream(copy):
                 copy.wait_event(done[cur])
                 hrho[cur].copy_(rho, non_blocking=True)

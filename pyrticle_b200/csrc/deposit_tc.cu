@@ -539,7 +539,7 @@ __device__ __forceinline__ void pad_chunk(Smem &S, int from, int to, int tid) {
 template <bool HITS>
 __device__ __forceinline__ uint32_t weights(uint32_t tmem, int warp, int lane) {
   const uint32_t base = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(64 * (warp >> 2));
-  uint32_t hits = 0;
+  float hits = 0;  // below 65: exact
 #pragma unroll 1
   for (int half = 0; half < 2; ++half) {
     uint32_t r[32];
@@ -549,13 +549,14 @@ __device__ __forceinline__ uint32_t weights(uint32_t tmem, int warp, int lane) {
     for (int i = 0; i < 32; ++i) {
       const float sc = __uint_as_float(r[i]);
       const float t = sc + fabsf(sc);                        // 2 max(s, 0), exact
-      r[i] = __float_as_uint(fmaf(t, t, 8388608.0f));        // 2^23 + round(t^2)
-      if (HITS) hits += r[i] != 0x4B000000u;
+      const float f = fmaf(t, t, 8388608.0f);                // 2^23 + round(t^2)
+      r[i] = __float_as_uint(f);
+      if (HITS) hits += __saturatef(f - 8388608.0f);         // F > 0: 1, else 0
     }
     tmem_st32(base + 32 * half, r);
   }
   tmem_wait_st();
-  return hits;
+  return (uint32_t)hits;
 }
 
 // Instruction descriptors (M = 128):
