@@ -462,13 +462,17 @@ __device__ __forceinline__ void cursor_init(const Smem &S, const TcArgs &A, Curs
 // Stages candidates into the ring until it holds `target` slots or every
 // warp's segments are exhausted (every fill warp; at most 32 slots per warp
 // past the target, so the ring holds at most target + 223).
+// The fill's per-tile constants: the cull box's half extents and squared
+// diameter (radius grown by 1e-5), 1/a and the bin width along x in FP32.
+struct FillConst {
+  float hf[3], rc4, inv_a, bw;
+};
+
 template <bool NORM>
-__device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const float hf[3], int target,
+__device__ __forceinline__ void fill(Smem &S, const TcArgs &A, const FillConst &F, int target,
                                      int lane, Cursor &C) {
-  const float rcf = (float)(A.radius * (1 + 1e-5));
-  const float rc4 = 4.0f * rcf * rcf;
-  const float inv_a = (float)A.inv_radius;
-  const float bw = (float)A.G.w[0];
+  const float *hf = F.hf;
+  const float rc4 = F.rc4, inv_a = F.inv_a, bw = F.bw;
   // culls batch B into the ring, then refills B with the warp's next batch
   auto process = [&](Batch &B) {
     const bool valid = lane < B.n;
@@ -596,12 +600,18 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   const uint32_t p0 = A.tile_starts[tile];
   const int npt = (int)(A.tile_starts[tile + 1] - p0);
   double c[3], hfd[3];
-  float hf[3];
+  FillConst fc;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     c[d] = A.tile_boxes[6 * tile + d];
     hfd[d] = A.tile_boxes[6 * tile + 3 + d] + 1e-5 * A.radius;
-    hf[d] = (float)hfd[d];
+    fc.hf[d] = (float)hfd[d];
+  }
+  {
+    const float rcf = (float)(A.radius * (1 + 1e-5));
+    fc.rc4 = 4.0f * rcf * rcf;
+    fc.inv_a = (float)A.inv_radius;
+    fc.bw = (float)A.G.w[0];
   }
 
   if (warp == 0) {
@@ -681,18 +691,22 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     tmem_wait_ld();
     const int cr = 32 * (warp & 3) + lane;
     if (cr < nvalid) {
-      // e_kk = 65536 D2 + 256 D1 + D0 (|e| < 2^38) for the six W digits kk:
-      // P = sum_kk 256^kk e_kk = Plo + 2^24 Phi (|Plo|, |Phi| < 2^55)
-      long long e[WDIG];
+      // P = sum_kk 256^kk (65536 D2 + 256 D1 + D0) over the six W digits kk
+      // = sum_j 256^j X_j with X_j = D0_j + D1_(j-1) + D2_(j-2) (|X| < 2^24,
+      // int32) = Plo + 2^32 Phi (Plo, Phi: four X each, |.| < 2^48)
+      int X[8];
 #pragma unroll
-      for (int kk = 0; kk < WDIG; ++kk)
-        e[kk] = 65536ll * (int)d2[kk] + 256ll * (int)d1[kk] + (long long)(int)d0[kk];
-      const long long plo = e[0] + e[1] * 256 + e[2] * 65536;
-      const long long phi = e[3] + e[4] * 256 + e[5] * 65536;
+      for (int j = 0; j < 8; ++j)
+        X[j] = (j <= 5 ? (int)d0[j] : 0) + (j >= 1 && j <= 6 ? (int)d1[j - 1] : 0) +
+               (j >= 2 ? (int)d2[j - 2] : 0);
+      const long long plo =
+          (long long)X[0] + 256ll * X[1] + 65536ll * X[2] + 16777216ll * X[3];
+      const long long phi =
+          (long long)X[4] + 256ll * X[5] + 65536ll * X[6] + 16777216ll * X[7];
       const long long M40 = (1ll << 40) - 1;
-      const long long l1 = (plo & M40) + ((phi & 0xffff) << 24);  // < 2^41
+      const long long l1 = (plo & M40) + ((phi & 0xff) << 32);  // < 2^41
       const long long L = l1 & M40;
-      const long long H = (plo >> 40) + (phi >> 16) + (l1 >> 40);
+      const long long H = (plo >> 40) + (phi >> 8) + (l1 >> 40);
       const uint32_t id = S.n.slot_id[(chunk * NC + cr) % RING];
       if (warp < 4) {
         if (H != 0) atomicAdd(A.norm_hi + id, (unsigned long long)H);
@@ -728,7 +742,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   int window = 0;       // chunks in the current int32 deposition window
   int valid_prev = 0;   // valid slots of the chunk whose accumulation is in flight
   if (ok) {
-    if (warp < FILL_WARPS) fill<NORM>(S, A, hf, NC, lane, cur);
+    if (warp < FILL_WARPS) fill<NORM>(S, A, fc, NC, lane, cur);
     __syncthreads();
     valid = min(S.tail, NC);
     if (valid > 0 && valid < NC) pad_chunk(S, valid, NC, tid);
@@ -749,7 +763,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     // (1) the fill warps stage chunk k+1 while the tensor cores score chunk
     // k and sum chunk k-1: the fill writes slots of chunks k+1 .. k+3 (at
     // most 223 past chunk k+1), never those of chunk k-1 (ring of five)
-    if (warp < FILL_WARPS) fill<NORM>(S, A, hf, (k + 2) * NC, lane, cur);
+    if (warp < FILL_WARPS) fill<NORM>(S, A, fc, (k + 2) * NC, lane, cur);
     // (2) the accumulation of chunk k-1 is complete: its weight digits may be
     // overwritten; read the normalisation sums, or fold a full window
     bool w = true;
