@@ -280,16 +280,33 @@ __device__ __forceinline__ uint32_t pack2(__half a, __half b) {
 //   [ux_h, ux_h, ux_l, uy_h, uy_h, uy_l, uz_h, uz_h, uz_l, b_h, b_l, 1, 1, 0, 0, 0]
 // with b = SIGMA (1 - |u|^2), so the product is
 //   u.v + b + g = SIGMA (1 - |u - w|^2) (up to the dropped low x low terms).
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+  return d;
+}
+
+__device__ __forceinline__ uint32_t h2bits(__half2 v) {
+  uint32_t u;
+  memcpy(&u, &v, sizeof(u));
+  return u;
+}
+
 __device__ __forceinline__ void candidate_operand(float w0, float w1, float w2, uint4 &k0,
                                                   uint4 &k1) {
-  __half h[3], l[3], gh, gl;
-  split_half(2.0f * SIGMA * w0, h[0], l[0]);
-  split_half(2.0f * SIGMA * w1, h[1], l[1]);
-  split_half(2.0f * SIGMA * w2, h[2], l[2]);
-  split_half(-SIGMA * fmaf(w0, w0, fmaf(w1, w1, w2 * w2)), gh, gl);
-  const __half one = __float2half_rn(1.0f), zero = __float2half_rn(0.0f);
-  k0 = make_uint4(pack2(h[0], l[0]), pack2(h[0], h[1]), pack2(l[1], h[1]), pack2(h[2], l[2]));
-  k1 = make_uint4(pack2(h[2], one), pack2(one, gh), pack2(gl, zero), pack2(zero, zero));
+  const float v0 = 2.0f * SIGMA * w0, v1 = 2.0f * SIGMA * w1, v2 = 2.0f * SIGMA * w2;
+  const float g = -SIGMA * fmaf(w0, w0, fmaf(w1, w1, w2 * w2));
+  // high FP16 terms of (v0, v1) and (v2, g) in pairs, then the low terms of
+  // the remainders (each value rounded to nearest, as one at a time)
+  const __half2 h01 = __floats2half2_rn(v0, v1), h2g = __floats2half2_rn(v2, g);
+  const float2 f01 = __half22float2(h01), f2g = __half22float2(h2g);
+  const uint32_t H01 = h2bits(h01), H2G = h2bits(h2g);
+  const uint32_t L01 = h2bits(__floats2half2_rn(v0 - f01.x, v1 - f01.y));
+  const uint32_t L2G = h2bits(__floats2half2_rn(v2 - f2g.x, g - f2g.y));
+  const uint32_t ONE = 0x3C00u;  // FP16 1.0
+  // [h0 l0 | h0 h1 | l1 h1 | h2 l2], [h2 1 | 1 gh | gl 0 | 0 0]
+  k0 = make_uint4(prmt(H01, L01, 0x5410), H01, prmt(L01, H01, 0x7632), prmt(H2G, L2G, 0x5410));
+  k1 = make_uint4((H2G & 0xffffu) | (ONE << 16), ONE | (H2G & 0xffff0000u), L2G >> 16, 0u);
 }
 
 // Bin-row segments of a tile (warp 0): every run of bins along x, in the
