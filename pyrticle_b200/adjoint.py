@@ -46,6 +46,15 @@ def _ptrs(tensors):
     return arr
 
 
+def _arg_key(a):
+    """A hashable value of a launch argument (pointer arrays as tuples)."""
+    if isinstance(a, C.Array):
+        return tuple(a)
+    if isinstance(a, C.c_void_p):
+        return a.value
+    return a
+
+
 def _field_components(f):
     """Six component tensors of a [6, Nn] field, None where identically zero."""
     return [f[k] if bool(torch.any(f[k] != 0)) else None for k in range(6)]
@@ -93,8 +102,12 @@ class DifferentiableTrajectory:
         self.c = method.units.VACUUM_LIGHT_SPEED()
         self.nn = len(method.discretization)
         # replay each segment's recomputation and adjoint launches from a
-        # CUDA graph captured on the first full segment
+        # CUDA graph captured on the first full segment; the graphs are kept
+        # across backward calls, keyed by every launch argument they hold
+        # (the caching allocator hands a repeated call the same buffers, so
+        # the capture happens once)
         self.use_graphs = True
+        self._graphs = {}
         # when True, backward_run records CUDA events between its phases
         # (launching every segment eagerly) and leaves the elapsed
         # milliseconds per phase in self.phase_ms
@@ -292,7 +305,7 @@ class DifferentiableTrajectory:
                            "prt_lsrk_stage_adjoint")
             self._mark(marks, "stage_adjoint")
 
-        graphs = {}
+        graphs = self._graphs
         self._mark(marks, "setup")
         for seg in reversed(range(len(cps))):
             xs, ps, els, order_s = cps[seg]
@@ -327,8 +340,12 @@ class DifferentiableTrajectory:
             if not self.use_graphs or self.time_phases or seg == len(cps) - 1:
                 segment(T)  # eager (the first one also sizes libprt's scratch)
                 continue
-            g = graphs.get(T)
+            key = (T, tuple(tuple(_arg_key(a) for a in args) for args in rec_args[:T]),
+                   tuple(tuple(_arg_key(a) for a in args) for args in adj_args[:T]))
+            g = graphs.get(key)
             if g is None:
+                if len(graphs) >= 8:
+                    graphs.clear()
                 # captured on a side stream with capture_begin/capture_end:
                 # the torch.cuda.graph context would also empty the caching
                 # allocator, making every later allocation a cudaMalloc
@@ -342,7 +359,7 @@ class DifferentiableTrajectory:
                     finally:
                         g.capture_end()
                 torch.cuda.current_stream().wait_stream(side)
-                graphs[T] = g
+                graphs[key] = g
             g.replay()
         meth.check_status()
         inv = torch.empty_like(cur_order)
