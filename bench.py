@@ -161,8 +161,8 @@ def timing_read(m, cat, reset=True):
 # profiles/dram_traffic_config2_16M.md); reported only for that workload.
 MEASURED_TRAFFIC = {
     "config2": {
-        "tc_deposit_kernel<0, 0>": 1486149120 + 120372992,
-        "tc_deposit_kernel<1, 1>": 1074607872 + 518718976,
+        "tc_deposit_kernel<0, 0>": 1486009600 + 119841792,
+        "tc_deposit_kernel<1, 1>": 1075521536 + 520001792,
         "deposit_groups_kernel<1, 1, 2>": 166834674176 + 130093312,
         "lsrk_stage_mixed_kernel<3>": 2012872448 + 1545450240,
     }
