@@ -51,6 +51,9 @@ def parse():
                          "default) or ShapeFunctionDepositor")
     ap.add_argument("--adjoint-scale", type=float, default=1.0,
                     help="particle-count scale of the differentiable workload (1M electrons)")
+    ap.add_argument("--adjoint-config4", type=float, default=None, metavar="SCALE",
+                    help="only the config4 adjoint (50 steps, checkpoint every 5) at this "
+                         "particle-count scale of its 64M; prints its own JSON line")
     return ap.parse_args()
 
 
@@ -655,6 +658,58 @@ def grid_bench(args, torch):
     print(json.dumps(line), flush=True)
 
 
+def adjoint_config4(torch, scale):
+    """config4's differentiable run: the 3,145,728-tet order-4 mesh, a Gaussian
+    bunch of 64M x scale electrons, 50 LSRK4 steps forward (chosen form:
+    mixed final deposition) and the adjoint with a checkpoint every 5 steps;
+    loss sum of j^2 (the workload has no field parameters). Reports the times
+    and the device memory in use after the forward and at the end of the
+    backward (cudaMemGetInfo: libprt's workspace and tapes included)."""
+    from pyrticle_b200 import problems
+    from pyrticle_b200.adjoint import DifferentiableTrajectory
+    w = problems.make("config4", scale=scale)
+    m, sf = build_method(w, torch)
+    dev = torch.device("cuda")
+    f64 = torch.float64
+    q = torch.as_tensor(w.charges, dtype=f64, device=dev)
+    mass = torch.as_tensor(w.masses, dtype=f64, device=dev)
+    x0 = torch.as_tensor(w.positions.T.copy(), dtype=f64, device=dev).contiguous()
+    p0 = torch.as_tensor(w.momenta.T.copy(), dtype=f64, device=dev).contiguous()
+    fields = torch.as_tensor(w.fields, dtype=f64, device=dev).contiguous()
+    traj = DifferentiableTrajectory(m, q, mass, w.dt, w.steps, 5, precision="mixed")
+    total = torch.cuda.mem_get_info()[1]
+
+    def used():
+        free, tot = torch.cuda.mem_get_info()
+        return tot - free
+
+    out = {}
+    for rep in range(2):  # the first call sizes the buffers and captures the graphs
+        p = p0.clone().requires_grad_()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        e[0].record()
+        _, j = traj(x0, p, None, fields)
+        L = (j ** 2).sum()
+        e[1].record()
+        torch.cuda.synchronize()
+        after_forward = used()
+        L.backward()
+        e[2].record()
+        torch.cuda.synchronize()
+        out = {"forward_ms": e[0].elapsed_time(e[1]), "backward_ms": e[1].elapsed_time(e[2]),
+               "device_bytes_after_forward": after_forward,
+               "device_bytes_end_of_backward": used()}
+        del p, j, L
+    out["ratio_backward_over_forward"] = out["backward_ms"] / out["forward_ms"]
+    line = {"metric": "adjoint backward / forward", "workload":
+            f"config4: {w.mesh.element_count} tets order {w.order}, {len(w.positions)} "
+            f"electrons ({scale:g} x 64M), {w.steps} LSRK4 steps, checkpoint every 5 steps "
+            "with recomputation, loss sum j^2, chosen form (mixed final deposition)",
+            "device_bytes_total": total, **out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -665,6 +720,9 @@ def main():
 
     if args.workload == "config1":
         grid_bench(args, torch)
+        return
+    if args.adjoint_config4 is not None:
+        adjoint_config4(torch, args.adjoint_config4)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
