@@ -170,14 +170,50 @@ __device__ __forceinline__ void mma_f16(uint32_t d, uint64_t a, uint64_t b, uint
       : "memory");
 }
 
-// int8 MMA with A in tensor memory (K-major: each 32-bit column holds four
-// consecutive K elements), B in shared memory
-__device__ __forceinline__ void mma_i8_ts(uint32_t d, uint32_t a_tmem, uint64_t b, uint32_t idesc,
-                                          uint32_t acc) {
+// The sums of one chunk: 16 int8 MMAs (K = 32 each) with A in tensor memory
+// (K-major: each 32-bit column holds four consecutive K elements) at columns
+// a0, a0 + 8, ... and B described by desc0, desc0 + 32 (512 bytes
+// further), ...; the first accumulates only if acc != 0, the rest always.
+// One statement, so the 16 issue back to back.
+__device__ __forceinline__ void mma_sums16(uint32_t d, uint32_t a0, uint64_t desc0,
+                                           uint32_t idesc, uint32_t acc) {
   asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d),
-      "r"(a_tmem), "l"(b), "r"(idesc), "r"(acc)
+      "{\n\t.reg .pred p, q;\n\t.reg .b64 d;\n\t.reg .b32 a;\n\t"
+      "setp.ne.b32 p, %3, 0;\n\tsetp.eq.b32 q, 0, 0;\n\t"
+      "mov.b64 d, %1;\n\tmov.b32 a, %2;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, p;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "add.s64 d, d, 32;\n\tadd.u32 a, a, 8;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [a], d, %4, q;\n\t"
+      "}\n"
+      ::"r"(d), "l"(desc0), "r"(a0), "r"(acc), "r"(idesc)
       : "memory");
 }
 
@@ -828,11 +864,9 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
       fence_after();
       const int slot0 = (k * NC) % RING;
       const uint32_t zb = z_dig + (NORM ? 0u : (uint32_t)(64 * slot0));
-#pragma unroll
-      for (int kk = 0; kk < NC / 8; ++kk)
-        mma_i8_ts(tmem + COL_ACC, tmem + (uint32_t)(8 * kk),
-                  sdesc(zb + (uint32_t)(16 * (32 * kk + 1)), 128, 16), IDESC_SUMS,
-                  (kk > 0 || (!NORM && window > 0)) ? 1u : 0u);
+      static_assert(NC / 8 == 16, "sixteen K steps per chunk");
+      mma_sums16(tmem + COL_ACC, tmem, sdesc(zb + 16u, 128, 16), IDESC_SUMS,
+                 (!NORM && window > 0) ? 1u : 0u);
       mma_commit(bar_a);
       if (valid_next > 0) {
         const int slot1 = ((k + 1) * NC) % RING;
