@@ -62,7 +62,11 @@
 // (mbarrier); one thread of a warp that stages nothing issues the
 // accumulation MMA of chunk k and then the score MMA of chunk k+1 (the MMAs
 // of one thread run in issue order, so the scores overwrite the weight words
-// only after the accumulation has read them). Every
+// only after the accumulation has read them), and one commit signals the
+// scores: it covers the accumulation issued before them too, so the sums of
+// chunk k-1 are read (or the next window's tiles reuse its ring slots) once
+// the scores of chunk k are ready; only the last chunk's sums have a commit
+// of their own. Every
 // mbarrier wait is bounded: a CTA whose wait runs out records PRT_ERR_TIMEOUT,
 // stops, waits (bounded) for its issued MMAs and frees its tensor memory.
 
@@ -793,6 +797,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
   const bool issuer = warp == ISSUE_WARP && lane == 0;
 
   int window = 0;       // chunks in the current int32 deposition window
+  int chunks = 0;       // chunks whose sums were issued
   int valid_prev = 0;   // valid slots of the chunk whose accumulation is in flight
   if (ok) {
     if (warp < FILL_WARPS) fill<NORM>(S, A, fc, NC, lane, cur);
@@ -817,14 +822,15 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     // k and sum chunk k-1: the fill writes slots of chunks k+1 .. k+3 (at
     // most 223 past chunk k+1), never those of chunk k-1 (ring of five)
     if (warp < FILL_WARPS) fill<NORM>(S, A, fc, (k + 2) * NC, lane, cur);
-    // (2) the accumulation of chunk k-1 is complete: its weight digits may be
-    // overwritten; read the normalisation sums, or fold a full window
-    bool w = true;
-    if (k > 0) {
-      w = mbar_wait(bar_a, (uint32_t)(waited_a & 1));
-      if (w) {
-        ++waited_a;
-        fence_after();
+    // (2) the scores of chunk k are ready, and with them the sums of chunk
+    // k-1 (the commit that signals the scores covers every MMA the issuing
+    // thread issued before them): read the normalisation sums, or fold a
+    // full window
+    bool w = mbar_wait(bar_s, (uint32_t)(waited_s & 1));
+    if (w) {
+      ++waited_s;
+      fence_after();
+      if (k > 0) {
         if (NORM) {
           norm_readout(k - 1, valid_prev);
         } else if (window == FLUSH_CHUNKS) {
@@ -832,13 +838,8 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
           window = 0;
         }
       }
-    }
-    // (3) the weights of chunk k
-    if (w) {
-      w = mbar_wait(bar_s, (uint32_t)(waited_s & 1));
-      if (w) {
-        ++waited_s;
-        fence_after();
+      // (3) the weights of chunk k
+      {
         const uint32_t h = weights<NORM && IND>(tmem, warp, lane);
         // the hits of this thread's candidate among its 64 positions, added
         // to the particle with the readout
@@ -867,15 +868,19 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
       static_assert(NC / 8 == 16, "sixteen K steps per chunk");
       mma_sums16(tmem + COL_ACC, tmem, sdesc(zb + 16u, 128, 16), IDESC_SUMS,
                  (!NORM && window > 0) ? 1u : 0u);
-      mma_commit(bar_a);
       if (valid_next > 0) {
         const int slot1 = ((k + 1) * NC) % RING;
         score_mma(slot1);
         mma_commit(bar_s);
+      } else {
+        mma_commit(bar_a);  // the last chunk's sums
       }
     }
-    ++issued_a;
-    if (valid_next > 0) ++issued_s;
+    if (valid_next > 0)
+      ++issued_s;
+    else
+      ++issued_a;
+    ++chunks;
     ++window;
     valid_prev = valid;
     valid = valid_next;
@@ -886,7 +891,7 @@ __global__ void __launch_bounds__(THREADS, 2) tc_deposit_kernel(TcArgs A) {
     if (ok) {
       fence_after();
       if (NORM)
-        norm_readout(issued_a - 1, valid_prev);
+        norm_readout(chunks - 1, valid_prev);
       else
         dep_fold();
     }
