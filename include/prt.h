@@ -221,10 +221,10 @@ enum prt_precision {
   /* chosen form. Stage: Lagrange values on the tensor cores (split BF16,
    * FP32 accumulation), force, update and locate in FP64. Deposition (shape
    * exponent 2): the weight max(1 - r^2/a^2, 0)^2 from a split-FP16
-   * tensor-core product with FP32 accumulation, rounded to a 16-bit integer,
-   * and summed exactly on the integer tensor cores against 48-bit integer
-   * charges (and 24-bit currents), combined into FP64 per node; the
-   * normalising integral per particle is summed exactly from the same
+   * tensor-core product with FP32 accumulation, rounded to a 23-bit integer,
+   * and summed exactly on the integer tensor cores against charges scaled to
+   * integers below 2^46 (currents below 2^22), combined into FP64 per node;
+   * the normalising integral per particle is summed exactly from the same
    * integer weights, so deposited charge matches the particles' charge to
    * FP64 rounding. Other exponents: as PRT_PRECISION_MIXED_SIMT. */
   PRT_PRECISION_MIXED = 1,

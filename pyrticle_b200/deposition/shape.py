@@ -28,8 +28,9 @@ class ShapeFunctionDepositor(Depositor):
 
     ``precision="fp64"`` is the plain form. ``"mixed"`` is the chosen form:
     on the tensor cores, the shape weights from a split-FP16 product rounded
-    to 16-bit integers and summed exactly against 48-bit integer charges
-    (24-bit currents), combined into FP64 per node; the normalising integral
+    to 23-bit integers and summed exactly against charges scaled to integers
+    below 2^46 (currents below 2^22), combined into FP64 per node; the
+    normalising integral
     is summed exactly from the same weights, so the normalised depositor's
     deposited charge equals the particles' charge to FP64 rounding.
     ``"mixed_simt"`` evaluates the weights and sums them in FP32 per batch of
